@@ -1,0 +1,333 @@
+"""Benchmark of the fused D3Q19 stream-collide step (GLUPS and % of HBM roofline).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--size L] [--precision fp64|fp32|fp16] [--scheme two_lattice|aa]
+
+Default workload: decaying HIT, 256^3 periodic box, FP64 two-lattice, tau = 0.505
+(svisc = 0.005/3), seeded random-phase solenoidal velocity with
+E(k) ~ k^4 exp(-2 (k/k0)^2), k0 = 4, u_rms = 0.03, equilibrium init. A step is
+one fused stream-collide update of the whole box (the reference's
+boundaries + col_MC). Prints one JSON line.
+
+- value: GLUPS with the populations resident in HBM, K steps timed with CUDA
+  events on the library's stream (inputs are 5 GB, larger than L2).
+- e2e: the same K steps through the public C-ABI as a user drives them: the
+  initial velocity field uploaded from pinned host memory, then
+  boundaries + col_MC + diagnostic every step (diagnostics computed every
+  icheck = 100 steps, the reference's default, SRC/input.F90:221, and read
+  back to the host), all inside the timed region.
+- roofline: algorithmic bytes of the stream-collide kernel (19 loads + 19
+  stores per cell) per launch / average launch time, against the measured HBM
+  copy bandwidth.
+- cpu_baseline: the CPU oracle (C restatement of the reference's
+  boundaries + col_MC, FP64, OpenMP over all host cores) on a bounded sample.
+- --impl reference: times that CPU implementation on this workload (rank 0).
+Under torchrun, each rank runs an independent replica box on its own GPU
+(the path needs no collective on one box per GPU); value is the sum of the
+ranks' cell updates over the slowest rank's time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+BYTES_PER_CELL = {"fp64": 304, "fp32": 152, "fp16": 76}
+DTYPE = {"fp64": "f64", "fp32": "f32", "fp16": "f16"}
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=400)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--size", type=int, default=256)
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32", "fp16"])
+    ap.add_argument("--scheme", default="two_lattice", choices=["two_lattice", "aa"])
+    ap.add_argument("--tau", type=float, default=0.505)
+    ap.add_argument("--k0", type=float, default=4.0)
+    ap.add_argument("--icheck", type=int, default=100)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    return ap.parse_args()
+
+
+def workload_name(a):
+    return (f"decaying HIT {a.size}^3 D3Q19 BGK, {a.precision} {a.scheme}, tau={a.tau}, k0={a.k0:g}, "
+            f"u_rms=0.03, seed 1234")
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("LOCAL_RANK", "0")), ws
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device, self.proc, self.path = device, None, None
+
+    def start(self):
+        try:
+            import tempfile
+
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "100",
+                 "-i", str(self.device)], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        pw = [float(r[3]) for r in rows if r[3].replace(".", "").isdigit()]
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows), "power_w_max": max(pw) if pw else None}
+
+
+# -------------------------------------------------------------- CPU oracle
+def cpu_baseline(a, seconds: float):
+    """The oracle's FP64 boundaries + col_MC (reference algorithm) on the host
+    cores, on the same box; steps sized to about `seconds` of CPU work."""
+    from oracle import oracle as O
+
+    O.set_num_threads(os.cpu_count() or 1)
+    L = a.size
+    orc = O.OracleLattice(L, L, L, form="f64")
+    from bgk3d_hit_b200.hit import hit_velocity
+
+    u, v, w = hit_velocity(L, a.k0, 0.03, 1234)
+    orc.init_velocity(u, v, w, 1.0)
+    svisc = (a.tau - 0.5) / 3.0
+    t1 = orc.time_steps(svisc, 1)
+    steps = max(1, min(200, int(seconds / max(t1, 1e-6))))
+    t = orc.time_steps(svisc, steps)
+    orc.close()
+    return {"value": L ** 3 * steps / t / 1e9, "unit": "GLUPS", "cores": O.num_threads(), "kind": "port",
+            "sample": f"{steps} steps of {L}^3 FP64 (step3 halo fill + col_MC, C restatement, OpenMP)"}
+
+
+def run_reference(a):
+    rank, _, ws = dist_env()
+    if rank != 0:
+        return
+    from oracle import oracle as O
+
+    O.set_num_threads(os.cpu_count() or 1)
+    L = a.size
+    from bgk3d_hit_b200.hit import hit_velocity
+
+    orc = O.OracleLattice(L, L, L, form="f64")
+    u, v, w = hit_velocity(L, a.k0, 0.03, 1234)
+    orc.init_velocity(u, v, w, 1.0)
+    svisc = (a.tau - 0.5) / 3.0
+    t1 = orc.time_steps(svisc, 1)
+    # each timed step is a bounded sample: cap the whole run at a few minutes
+    k = max(1, min(a.steps, int(120.0 / max(t1, 1e-6))))
+    w_ = max(0, min(a.warmup, 2))
+    orc.time_steps(svisc, w_)
+    t = orc.time_steps(svisc, k)
+    val = L ** 3 * k / t / 1e9
+    cores = O.num_threads()
+    line = {
+        "impl": "reference", "metric": "GLUPS (fused D3Q19 stream-collide)", "value": val, "unit": "GLUPS",
+        "n_gpus": ws, "steps": k, "warmup": w_, "ms_per_step": 1e3 * t / k, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": DTYPE["fp64"], "data": "synthetic",
+        "config": {"workload": workload_name(a), "box": L, "precision": "fp64", "scheme": "two_lattice"},
+        "cpu_baseline": {"value": val, "unit": "GLUPS", "cores": cores, "kind": "port",
+                         "sample": f"{k} steps of {L}^3 FP64, C restatement of boundaries + col_MC "
+                                   "(the Fortran/MPI reference cannot be built in this image)"},
+        "e2e": {"value": val, "unit": "GLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------------- GPU
+def measured_hbm():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        return float(json.load(open(p))["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def ncu_traffic(kernel_key: str):
+    p = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    try:
+        return json.load(open(p)).get(kernel_key)
+    except Exception:
+        return None
+
+
+def run_ours(a):
+    import torch
+
+    import bgk3d_hit_b200 as B
+    from bgk3d_hit_b200.hit import hit_velocity
+
+    rank, local, ws = dist_env()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+
+    L = a.size
+    svisc = (a.tau - 0.5) / 3.0
+    u, v, w = hit_velocity(L, a.k0, 0.03, 1234)
+    pin = [torch.from_numpy(x).pin_memory() for x in (u, v, w)]
+    box = B.BGK3D(L, svisc=svisc, u0=0.03, precision=a.precision, scheme=a.scheme, icheck=a.icheck, device=local)
+    box.init_velocity(*(p.numpy() for p in pin))
+    stream = torch.cuda.ExternalStream(box.stream, device=local)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if ws > 1:
+            torch.distributed.barrier()
+        box.synchronize()
+
+    def max_over_ranks(x: float) -> float:
+        if ws == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item())
+
+    # warm-up
+    box.run(a.warmup)
+    barrier()
+    # -------- timed: K fused steps, populations resident
+    clocks = ClockSampler(local)
+    clocks.start()
+    l0 = box.launch_count
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    e0.record(stream)
+    box.run(a.steps)
+    e1.record(stream)
+    barrier()
+    ms = e0.elapsed_time(e1)
+    launches = box.launch_count - l0
+    clk = clocks.stop()
+    ms_max = max_over_ranks(ms)
+    lu = float(L) ** 3 * a.steps
+    value = ws * lu / (ms_max * 1e-3) / 1e9
+    per_launch_s = ms * 1e-3 / a.steps
+    bpc = BYTES_PER_CELL[a.precision]
+    achieved = bpc * float(L) ** 3 / per_launch_s / 1e9
+    peak, peak_kind = measured_hbm()
+    kern = f"{'k_two' if a.scheme == 'two_lattice' else 'k_aa'}_{a.precision}"
+    tr = ncu_traffic(kern)
+    traffic = tr * float(L) ** 3 if tr else None
+
+    # -------- e2e through the C-ABI with host buffers
+    e2e = None
+    if not a.no_e2e:
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        box2 = B.BGK3D(L, svisc=svisc, u0=0.03, precision=a.precision, scheme=a.scheme, icheck=a.icheck,
+                       device=local)
+        stream2 = torch.cuda.ExternalStream(box2.stream, device=local)
+        torch.cuda.synchronize()
+        if ws > 1:
+            torch.distributed.barrier()
+        t0 = time.perf_counter()
+        ev0.record(stream2)
+        box2.init_velocity(*(p.numpy() for p in pin))
+        ndiag = 0
+        for it in range(1, a.steps + 1):
+            box2.boundaries(it)
+            box2.col_MC(it)
+            if box2.diagnostic(it) is not None or it == a.steps:
+                ndiag += 1
+        if a.steps % a.icheck:
+            box2.diagno(a.steps)
+        ev1.record(stream2)
+        box2.synchronize()
+        wall = time.perf_counter() - t0
+        ms2 = max_over_ranks(max(ev0.elapsed_time(ev1), 1e3 * wall))
+        diag_bytes = 11 * 8
+        e2e = {"value": ws * lu / (ms2 * 1e-3) / 1e9, "unit": "GLUPS",
+               "h2d_bytes_per_step": int(3 * 8 * L ** 3 / a.steps),
+               "d2h_bytes_per_step": int(diag_bytes * ndiag / a.steps),
+               "includes": f"velocity upload from pinned host memory, {a.steps} x (boundaries + col_MC + "
+                           f"diagnostic gated by icheck={a.icheck}), diagnostics read back"}
+        box2.close()
+
+    cpu = None
+    if rank == 0 and ws == 1 and not a.no_cpu:
+        try:
+            cpu = cpu_baseline(a, a.cpu_seconds)
+        except Exception as ex:  # the checker is optional for the GPU number
+            cpu = {"value": None, "unit": "GLUPS", "cores": os.cpu_count(), "kind": "port", "sample": f"failed: {ex}"}
+
+    if rank == 0:
+        line = {
+            "metric": "GLUPS (fused D3Q19 stream-collide)", "value": value, "unit": "GLUPS", "n_gpus": ws,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_max / a.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": DTYPE[a.precision], "data": "synthetic",
+            "config": {"workload": workload_name(a), "box": L, "precision": a.precision, "scheme": a.scheme,
+                       "tau": a.tau, "cells_per_gpu": L ** 3,
+                       "l2": f"inputs larger than L2 ({box.device_bytes / 1e9:.1f} GB resident, L2 126 MB)",
+                       "parallelism": f"{ws} independent replica box(es), one per GPU"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "peak_kind": peak_kind, "bytes_per_cell": bpc, "kernel": kern},
+            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    box.close()
+    if ws > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_ours(a)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,738 @@
+// C-ABI of the library (include/bgk3d.h): context, parameter checks, device
+// memory, and the reference's call sequence mapped onto the kernels.
+#include <cuda_runtime.h>
+#include <cufft.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "bgk3d.h"
+#include "kernels.h"
+
+using namespace bgk;
+
+namespace {
+
+thread_local char g_err[512] = "";
+
+void set_err(const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+  set_err("%s: %s", what, cudaGetErrorString(e));
+  return e == cudaErrorMemoryAllocation ? BGK_ERR_NOMEM : BGK_ERR_CUDA;
+}
+
+#define CK(call)                                         \
+  do {                                                   \
+    cudaError_t e_ = (call);                             \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #call);  \
+  } while (0)
+
+// Rows are padded to a multiple of 32 elements so that every row starts on a
+// 64..256-byte boundary; populations start on 256-element boundaries.
+constexpr int ROW_ALIGN = 32;
+constexpr long long POP_ALIGN = 256;
+// Staging for host velocity input: this many cells per chunk (whole planes).
+constexpr long long INIT_CHUNK_CELLS = 1LL << 24;
+
+}  // namespace
+
+struct bgk_ctx {
+  bgk_params p;
+  int form = 0, scheme = 0;
+  cudaStream_t st = nullptr;
+  Geo g{};
+  size_t es = 8;
+  void* memA = nullptr;
+  void* memB = nullptr;
+  Lattice A{}, B{};
+  int lay = LAY_TWO;
+  int initialized = 0;
+  long long step = 0;
+  double omega = 0.0, scale = 1.0;
+  double* partials = nullptr;
+  double* totals = nullptr;
+  double* h_tot = nullptr;  // pinned
+  unsigned int* d_max = nullptr;
+  void* vel = nullptr;
+  void* stage = nullptr;
+  size_t stage_bytes = 0;
+  long long launches = 0;
+  long long dev_bytes = 0;
+  void* fft_buf = nullptr;
+  size_t fft_bytes = 0;
+  cufftHandle plan = 0;
+  int plan_ok = 0;
+  double* d_bins = nullptr;
+  int nbins_alloc = 0;
+};
+
+namespace {
+
+long long ncell(const bgk_ctx* c) { return (long long)c->g.nx * c->g.ny * c->g.nz; }
+size_t rsize(const bgk_ctx* c) { return c->form == FORM_F64 ? 8 : 4; }
+
+int dev_alloc(bgk_ctx* c, void** ptr, size_t bytes, const char* what) {
+  cudaError_t e = cudaMalloc(ptr, bytes);
+  if (e != cudaSuccess) {
+    (void)cudaGetLastError();
+    *ptr = nullptr;
+    set_err("cudaMalloc(%zu bytes) for %s: %s", bytes, what, cudaGetErrorString(e));
+    return e == cudaErrorMemoryAllocation ? BGK_ERR_NOMEM : BGK_ERR_CUDA;
+  }
+  c->dev_bytes += (long long)bytes;
+  return BGK_OK;
+}
+
+int ensure_stage(bgk_ctx* c, size_t bytes) {
+  if (c->stage_bytes >= bytes) return BGK_OK;
+  if (c->stage) {
+    CK(cudaStreamSynchronize(c->st));
+    cudaFree(c->stage);
+    c->dev_bytes -= (long long)c->stage_bytes;
+    c->stage = nullptr;
+    c->stage_bytes = 0;
+  }
+  int rc = dev_alloc(c, &c->stage, bytes, "staging buffer");
+  if (rc) return rc;
+  c->stage_bytes = bytes;
+  return BGK_OK;
+}
+
+int ensure_vel(bgk_ctx* c) {
+  if (c->vel) return BGK_OK;
+  return dev_alloc(c, &c->vel, 3 * (size_t)ncell(c) * rsize(c), "velocity field");
+}
+
+int check_ctx(const bgk_ctx* c) {
+  if (!c) {
+    set_err("null context");
+    return BGK_ERR_INVALID;
+  }
+  return BGK_OK;
+}
+
+int check_init(bgk_ctx* c) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!c->initialized) {
+    set_err("populations not initialised (call bgk_init_tgv, bgk_init_velocity or bgk_put_populations)");
+    return BGK_ERR_STATE;
+  }
+  return BGK_OK;
+}
+
+// omega = (uno+uno)/((6.0*svisc)+1.0), SRC/hencol.F90:31, in the arithmetic
+// type of the form (volatile keeps each rounding as written).
+double omega_of(const bgk_params& p, int form) {
+  if (p.use_omega) return p.omega;
+  if (form == FORM_F64) {
+    volatile double s = p.svisc;
+    volatile double a = 6.0 * s;
+    volatile double b = a + 1.0;
+    return (1.0 + 1.0) / b;
+  }
+  volatile float s = (float)p.svisc;
+  volatile float a = 6.0f * s;
+  volatile float b = a + 1.0f;
+  volatile float o = (1.0f + 1.0f) / b;
+  return (double)o;
+}
+
+// Smallest-exponent-headroom scale for the FP16 form:
+// 2^floor(log2(65504 / (4 max|f - w|))).
+double fp16_scale_for(float maxabs) {
+  if (!(maxabs > 0.f) || !std::isfinite(maxabs)) return 1.0;
+  const double r = 65504.0 / (4.0 * (double)maxabs);
+  return std::ldexp(1.0, (int)std::floor(std::log2(r)));
+}
+
+int set_scale_from_max(bgk_ctx* c) {
+  unsigned int bits = 0;
+  CK(cudaMemcpyAsync(&bits, c->d_max, sizeof(bits), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  float m;
+  std::memcpy(&m, &bits, sizeof(m));
+  c->scale = fp16_scale_for(m);
+  return BGK_OK;
+}
+
+int init_layout(const bgk_ctx* c) { return c->scheme == BGK_AA ? LAY_AAE : LAY_TWO; }
+
+int compute_diag(bgk_ctx* c, int itime, bgk_diag* out, int want_extras) {
+  const bool extras = want_extras && c->p.extras;
+  if (extras) {
+    int rc = ensure_vel(c);
+    if (rc) return rc;
+  }
+  CK(launch_diag(c->A, c->lay, c->p.svisc, c->omega, c->scale, c->partials, extras ? c->vel : nullptr, c->st));
+  c->launches++;
+  if (extras) {
+    CK(launch_enstrophy(c->A, c->vel, c->partials, c->st));
+    c->launches++;
+  }
+  CK(launch_finalize(c->partials, c->totals, c->st));
+  c->launches++;
+  const bool faithful = c->p.mode == BGK_FAITHFUL;
+  if (faithful) {
+    CK(launch_last_zj(c->A, c->lay, c->scale, c->totals + ND, c->st));
+    c->launches++;
+  }
+  CK(cudaMemcpyAsync(c->h_tot, c->totals, (ND + 1) * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  const double* t = c->h_tot;
+  const double N = (double)ncell(c);
+  out->itime = itime;
+  out->rho_mean = t[0] / N;
+  out->ux_mean = t[1] / N;
+  out->uy_mean = t[2] / N;
+  // SRC/diagno.F90:110 accumulates ztot = ytot + zj: the final value is the
+  // full y sum plus zj of the last cell.
+  out->uz_mean = faithful ? (t[2] + t[ND]) / N : t[3] / N;
+  out->ke_mean = t[4] / N;
+  // t = float(itime)*dt with dx = (2.0*3.141592)/float(lx) in single precision
+  // and dt = dx*u0 (SRC/dissipation.F90:65-66,262), in the form's arithmetic.
+  const float dxs = (2.0f * 3.141592f) / (float)c->g.nx;
+  double u0r;
+  if (c->form == FORM_F64) {
+    volatile double dt = (double)dxs * c->p.u0;
+    out->t = (double)(float)itime * dt;
+    u0r = c->p.u0;
+  } else {
+    volatile float dt = dxs * (float)c->p.u0;
+    volatile float tt = (float)itime * dt;
+    out->t = (double)tt;
+    u0r = (double)(float)c->p.u0;
+  }
+  out->tke = t[5];
+  out->tke_norm = t[5] / (double)c->g.nx / (double)c->g.ny / (double)c->g.nz / (u0r * u0r);
+  out->diss = t[6];
+  out->eps_strain = t[7] / N;
+  out->nonfinite = (long long)t[8];
+  out->enstrophy = extras ? t[9] / N : 0.0;
+  if (out->nonfinite > 0) {
+    set_err("diagnostics: %lld cells with non-finite density or velocity at itime %d", out->nonfinite, itime);
+    return BGK_ERR_NONFINITE;
+  }
+  return BGK_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int bgk_params_default(bgk_params* p) {
+  if (!p) return BGK_ERR_INVALID;
+  std::memset(p, 0, sizeof(*p));
+  p->lx = p->ly = p->lz = 64;
+  p->svisc = 0.01;
+  p->u0 = 0.05;
+  p->precision = BGK_FP64;
+  p->scheme = BGK_TWO_LATTICE;
+  p->icheck = 10;
+  p->mode = BGK_CORRECTED;
+  p->fp16_scale = 0.0;
+  p->device = 0;
+  p->use_omega = 0;
+  p->omega = 0.0;
+  p->extras = 1;
+  return BGK_OK;
+}
+
+int bgk_create(const bgk_params* p, bgk_ctx** out) {
+  if (!p || !out) {
+    set_err("null argument");
+    return BGK_ERR_INVALID;
+  }
+  *out = nullptr;
+  // parameter checks (the reference stops on inconsistent sizes,
+  // SRC/input.F90:66-82; here every check returns an error instead)
+  if (p->lx < 1 || p->ly < 1 || p->lz < 1 || p->lz > 65535) {
+    set_err("invalid box %d x %d x %d", p->lx, p->ly, p->lz);
+    return BGK_ERR_INVALID;
+  }
+  if (p->precision < BGK_FP64 || p->precision > BGK_FP16DEV) {
+    set_err("invalid precision %d", p->precision);
+    return BGK_ERR_INVALID;
+  }
+  if (p->scheme != BGK_TWO_LATTICE && p->scheme != BGK_AA) {
+    set_err("invalid scheme %d", p->scheme);
+    return BGK_ERR_INVALID;
+  }
+  if (p->mode != BGK_CORRECTED && p->mode != BGK_FAITHFUL) {
+    set_err("invalid mode %d", p->mode);
+    return BGK_ERR_INVALID;
+  }
+  if (p->icheck < 1) {
+    set_err("icheck must be >= 1 (got %d)", p->icheck);
+    return BGK_ERR_INVALID;
+  }
+  if (p->use_omega) {
+    if (!(p->omega >= 0.0 && p->omega <= 2.0)) {
+      set_err("omega override %g outside [0, 2]", p->omega);
+      return BGK_ERR_INVALID;
+    }
+  } else if (!(p->svisc > 0.0) || !std::isfinite(p->svisc)) {
+    set_err("svisc must be > 0 (tau = 3 svisc + 1/2 > 1/2), got %g", p->svisc);
+    return BGK_ERR_INVALID;
+  }
+  if (!std::isfinite(p->u0)) {
+    set_err("u0 must be finite");
+    return BGK_ERR_INVALID;
+  }
+  if (p->fp16_scale != 0.0) {
+    int ex;
+    const double m = std::frexp(p->fp16_scale, &ex);
+    if (!(p->fp16_scale > 0.0) || m != 0.5) {
+      set_err("fp16_scale must be 0 or a positive power of two, got %g", p->fp16_scale);
+      return BGK_ERR_INVALID;
+    }
+  }
+  const long long sx = ((long long)p->lx + ROW_ALIGN - 1) / ROW_ALIGN * ROW_ALIGN;
+  const long long cells = sx * p->ly * p->lz;
+  if (cells >= (1LL << 31) - POP_ALIGN) {
+    set_err("box too large: %lld padded cells per population (limit 2^31)", cells);
+    return BGK_ERR_INVALID;
+  }
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev == 0) {
+    set_err("no CUDA device: %s", cudaGetErrorString(e));
+    return BGK_ERR_CUDA;
+  }
+  if (p->device < 0 || p->device >= ndev) {
+    set_err("device %d out of range (%d devices)", p->device, ndev);
+    return BGK_ERR_INVALID;
+  }
+  CK(cudaSetDevice(p->device));
+
+  bgk_ctx* c = new bgk_ctx();
+  c->p = *p;
+  c->form = p->precision;
+  c->scheme = p->scheme;
+  c->es = c->form == FORM_F64 ? 8 : (c->form == FORM_F32 ? 4 : 2);
+  c->g.nx = p->lx;
+  c->g.ny = p->ly;
+  c->g.nz = p->lz;
+  c->g.sx = (int)sx;
+  c->g.qs = (cells + POP_ALIGN - 1) / POP_ALIGN * POP_ALIGN;
+  c->omega = omega_of(*p, c->form);
+  c->scale = c->form == FORM_F16 ? (p->fp16_scale != 0.0 ? p->fp16_scale : 1.0) : 1.0;
+  c->A.form = c->B.form = c->form;
+  c->A.g = c->B.g = c->g;
+
+  auto fail = [&](int rc) {
+    bgk_destroy(c);
+    return rc;
+  };
+  e = cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking);
+  if (e != cudaSuccess) return fail(cuda_fail(e, "cudaStreamCreate"));
+  const size_t pop_bytes = (size_t)c->g.qs * c->es;
+  int rc = dev_alloc(c, &c->memA, Q * pop_bytes, "lattice a");
+  if (rc) return fail(rc);
+  for (int q = 0; q < Q; ++q) c->A.p[q] = (char*)c->memA + q * pop_bytes;
+  if (c->scheme == BGK_TWO_LATTICE) {
+    // b01..b18; b19 is never used (pop 19 is updated in place,
+    // SRC/col_MC.F90:351), so it is not allocated
+    rc = dev_alloc(c, &c->memB, (Q - 1) * pop_bytes, "lattice b");
+    if (rc) return fail(rc);
+    for (int q = 0; q < Q - 1; ++q) c->B.p[q] = (char*)c->memB + q * pop_bytes;
+    c->B.p[Q - 1] = c->A.p[Q - 1];
+  }
+  rc = dev_alloc(c, (void**)&c->partials, (size_t)DIAG_BLOCKS * ND * 2 * sizeof(double), "diagnostic partials");
+  if (rc) return fail(rc);
+  rc = dev_alloc(c, (void**)&c->totals, (ND + 1) * sizeof(double), "diagnostic totals");
+  if (rc) return fail(rc);
+  rc = dev_alloc(c, (void**)&c->d_max, sizeof(unsigned int), "scale probe");
+  if (rc) return fail(rc);
+  e = cudaMallocHost((void**)&c->h_tot, (ND + 1) * sizeof(double));
+  if (e != cudaSuccess) return fail(cuda_fail(e, "cudaMallocHost"));
+  c->lay = init_layout(c);
+  *out = c;
+  return BGK_OK;
+}
+
+int bgk_destroy(bgk_ctx* c) {
+  if (!c) return BGK_OK;
+  cudaSetDevice(c->p.device);
+  if (c->st) cudaStreamSynchronize(c->st);
+  if (c->plan_ok) cufftDestroy(c->plan);
+  cudaFree(c->memA);
+  cudaFree(c->memB);
+  cudaFree(c->partials);
+  cudaFree(c->totals);
+  cudaFree(c->d_max);
+  cudaFree(c->vel);
+  cudaFree(c->stage);
+  cudaFree(c->fft_buf);
+  cudaFree(c->d_bins);
+  if (c->h_tot) cudaFreeHost(c->h_tot);
+  if (c->st) cudaStreamDestroy(c->st);
+  delete c;
+  return BGK_OK;
+}
+
+int bgk_init_tgv(bgk_ctx* c) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  CK(cudaSetDevice(c->p.device));
+  const int lay = init_layout(c);
+  const int faithful = c->p.mode == BGK_FAITHFUL;
+  if (c->form == FORM_F16 && c->p.fp16_scale == 0.0) {
+    CK(cudaMemsetAsync(c->d_max, 0, sizeof(unsigned int), c->st));
+    CK(launch_init_tgv(c->A, lay, c->p.u0, faithful, 1.0, c->d_max, c->st));
+    c->launches++;
+    rc = set_scale_from_max(c);
+    if (rc) return rc;
+  }
+  CK(launch_init_tgv(c->A, lay, c->p.u0, faithful, c->scale, nullptr, c->st));
+  c->launches++;
+  c->lay = lay;
+  c->step = 0;
+  c->initialized = 1;
+  return BGK_OK;
+}
+
+int bgk_init_velocity(bgk_ctx* c, const double* u, const double* v, const double* w, double rho) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!u || !v || !w) {
+    set_err("null velocity array");
+    return BGK_ERR_INVALID;
+  }
+  if (!(rho > 0.0) || !std::isfinite(rho)) {
+    set_err("rho must be positive and finite, got %g", rho);
+    return BGK_ERR_INVALID;
+  }
+  CK(cudaSetDevice(c->p.device));
+  const long long plane = (long long)c->g.nx * c->g.ny;
+  int nk = (int)(INIT_CHUNK_CELLS / plane);
+  if (nk < 1) nk = 1;
+  if (nk > c->g.nz) nk = c->g.nz;
+  const size_t chunk = (size_t)plane * nk;
+  rc = ensure_stage(c, 3 * chunk * sizeof(double));
+  if (rc) return rc;
+  double* su = (double*)c->stage;
+  double* sv = su + chunk;
+  double* sw = sv + chunk;
+  const int lay = init_layout(c);
+  const bool measure = c->form == FORM_F16 && c->p.fp16_scale == 0.0;
+  if (measure) CK(cudaMemsetAsync(c->d_max, 0, sizeof(unsigned int), c->st));
+  for (int pass = measure ? 0 : 1; pass < 2; ++pass) {
+    if (pass == 1 && measure) {
+      rc = set_scale_from_max(c);
+      if (rc) return rc;
+    }
+    for (int k0 = 0; k0 < c->g.nz; k0 += nk) {
+      const int nkk = k0 + nk <= c->g.nz ? nk : c->g.nz - k0;
+      const size_t off = (size_t)plane * k0, cnt = (size_t)plane * nkk * sizeof(double);
+      CK(cudaMemcpyAsync(su, u + off, cnt, cudaMemcpyHostToDevice, c->st));
+      CK(cudaMemcpyAsync(sv, v + off, cnt, cudaMemcpyHostToDevice, c->st));
+      CK(cudaMemcpyAsync(sw, w + off, cnt, cudaMemcpyHostToDevice, c->st));
+      CK(launch_init_velocity(c->A, lay, su, sv, sw, rho, k0, nkk, pass == 0 ? 1.0 : c->scale,
+                              pass == 0 ? c->d_max : nullptr, c->st));
+      c->launches++;
+    }
+  }
+  CK(cudaStreamSynchronize(c->st));
+  c->lay = lay;
+  c->step = 0;
+  c->initialized = 1;
+  return BGK_OK;
+}
+
+int bgk_boundaries(bgk_ctx* c, int itime) {
+  (void)itime;
+  return check_ctx(c);
+}
+
+int bgk_col_mc(bgk_ctx* c, int itime) {
+  (void)itime;
+  int rc = check_init(c);
+  if (rc) return rc;
+  CK(cudaSetDevice(c->p.device));
+  if (c->scheme == BGK_TWO_LATTICE) {
+    CK(launch_two_lattice(c->A, c->B, c->omega, c->scale, 0, c->st));
+    // pointer swap of pops 01..18, SRC/col_MC.F90:364-421
+    for (int q = 0; q < Q - 1; ++q) {
+      void* t = c->A.p[q];
+      c->A.p[q] = c->B.p[q];
+      c->B.p[q] = t;
+    }
+  } else {
+    const int odd = c->lay == LAY_AAE;
+    CK(launch_aa(c->A, odd, c->omega, c->scale, c->st));
+    c->lay = odd ? LAY_AAN : LAY_AAE;
+  }
+  c->launches++;
+  c->step++;
+  return BGK_OK;
+}
+
+int bgk_run(bgk_ctx* c, int nsteps) {
+  if (nsteps < 0) {
+    set_err("nsteps < 0");
+    return BGK_ERR_INVALID;
+  }
+  for (int s = 0; s < nsteps; ++s) {
+    int rc = bgk_boundaries(c, (int)(c ? c->step + 1 : 0));
+    if (rc) return rc;
+    rc = bgk_col_mc(c, (int)(c->step + 1));
+    if (rc) return rc;
+  }
+  return BGK_OK;
+}
+
+int bgk_diagnostic(bgk_ctx* c, int itime, bgk_diag* out) {
+  int rc = check_init(c);
+  if (rc) return rc;
+  if (!out) {
+    set_err("null output");
+    return BGK_ERR_INVALID;
+  }
+  if (itime % c->p.icheck != 0) return BGK_SKIPPED;  // SRC/diagnostic.F90:37
+  CK(cudaSetDevice(c->p.device));
+  return compute_diag(c, itime, out, 1);
+}
+
+int bgk_diagno(bgk_ctx* c, int itime, double* o) {
+  int rc = check_init(c);
+  if (rc) return rc;
+  if (!o) return BGK_ERR_INVALID;
+  CK(cudaSetDevice(c->p.device));
+  bgk_diag d;
+  rc = compute_diag(c, itime, &d, 0);
+  if (rc && rc != BGK_ERR_NONFINITE) return rc;
+  o[0] = d.rho_mean; o[1] = d.ux_mean; o[2] = d.uy_mean; o[3] = d.uz_mean; o[4] = d.ke_mean;
+  return rc;
+}
+
+int bgk_dissipation(bgk_ctx* c, int itime, double* o) {
+  int rc = check_init(c);
+  if (rc) return rc;
+  if (!o) return BGK_ERR_INVALID;
+  CK(cudaSetDevice(c->p.device));
+  bgk_diag d;
+  rc = compute_diag(c, itime, &d, 0);
+  if (rc && rc != BGK_ERR_NONFINITE) return rc;
+  o[0] = d.t; o[1] = d.tke_norm; o[2] = d.diss; o[3] = d.tke;
+  return rc;
+}
+
+int bgk_get_populations(bgk_ctx* c, void* host) {
+  int rc = check_init(c);
+  if (rc) return rc;
+  if (!host) return BGK_ERR_INVALID;
+  CK(cudaSetDevice(c->p.device));
+  const size_t n = (size_t)ncell(c);
+  rc = ensure_stage(c, n * 8);
+  if (rc) return rc;
+  for (int q = 0; q < Q; ++q) {
+    CK(launch_export(c->A, c->lay, q, c->stage, nullptr, c->scale, c->st));
+    c->launches++;
+    CK(cudaMemcpyAsync((char*)host + q * n * c->es, c->stage, n * c->es, cudaMemcpyDeviceToHost, c->st));
+  }
+  CK(cudaStreamSynchronize(c->st));
+  return BGK_OK;
+}
+
+int bgk_get_deviations(bgk_ctx* c, double* host) {
+  int rc = check_init(c);
+  if (rc) return rc;
+  if (!host) return BGK_ERR_INVALID;
+  CK(cudaSetDevice(c->p.device));
+  const size_t n = (size_t)ncell(c);
+  rc = ensure_stage(c, n * 8);
+  if (rc) return rc;
+  for (int q = 0; q < Q; ++q) {
+    CK(launch_export(c->A, c->lay, q, nullptr, (double*)c->stage, c->scale, c->st));
+    c->launches++;
+    CK(cudaMemcpyAsync(host + q * n, c->stage, n * 8, cudaMemcpyDeviceToHost, c->st));
+  }
+  CK(cudaStreamSynchronize(c->st));
+  return BGK_OK;
+}
+
+int bgk_put_populations(bgk_ctx* c, const void* host) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!host) return BGK_ERR_INVALID;
+  CK(cudaSetDevice(c->p.device));
+  const size_t n = (size_t)ncell(c);
+  rc = ensure_stage(c, n * 8);
+  if (rc) return rc;
+  const int lay = c->initialized ? c->lay : init_layout(c);
+  for (int q = 0; q < Q; ++q) {
+    CK(cudaMemcpyAsync(c->stage, (const char*)host + q * n * c->es, n * c->es, cudaMemcpyHostToDevice, c->st));
+    CK(launch_import(c->A, lay, q, c->stage, c->st));
+    c->launches++;
+  }
+  CK(cudaStreamSynchronize(c->st));
+  c->lay = lay;
+  if (!c->initialized) c->step = 0;
+  c->initialized = 1;
+  return BGK_OK;
+}
+
+int bgk_get_velocity(bgk_ctx* c, double* u, double* v, double* w) {
+  int rc = check_init(c);
+  if (rc) return rc;
+  if (!u || !v || !w) return BGK_ERR_INVALID;
+  CK(cudaSetDevice(c->p.device));
+  rc = ensure_vel(c);
+  if (rc) return rc;
+  CK(launch_diag(c->A, c->lay, c->p.svisc, c->omega, c->scale, c->partials, c->vel, c->st));
+  c->launches++;
+  const size_t n = (size_t)ncell(c);
+  double* dst[3] = {u, v, w};
+  if (c->form == FORM_F64) {
+    for (int d = 0; d < 3; ++d)
+      CK(cudaMemcpyAsync(dst[d], (double*)c->vel + d * n, n * 8, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+  } else {
+    std::vector<float> tmp(n);
+    for (int d = 0; d < 3; ++d) {
+      CK(cudaMemcpyAsync(tmp.data(), (float*)c->vel + d * n, n * 4, cudaMemcpyDeviceToHost, c->st));
+      CK(cudaStreamSynchronize(c->st));
+      for (size_t s = 0; s < n; ++s) dst[d][s] = (double)tmp[s];
+    }
+  }
+  return BGK_OK;
+}
+
+int bgk_spectrum(bgk_ctx* c, int nbins, double* ek) {
+  int rc = check_init(c);
+  if (rc) return rc;
+  if (!ek || nbins < 1) {
+    set_err("bgk_spectrum: invalid argument");
+    return BGK_ERR_INVALID;
+  }
+  CK(cudaSetDevice(c->p.device));
+  rc = ensure_vel(c);
+  if (rc) return rc;
+  CK(launch_diag(c->A, c->lay, c->p.svisc, c->omega, c->scale, c->partials, c->vel, c->st));
+  c->launches++;
+  const int nx = c->g.nx, ny = c->g.ny, nz = c->g.nz;
+  const size_t cplx = (size_t)nz * ny * (nx / 2 + 1);
+  const bool dbl = c->form == FORM_F64;
+  if (!c->fft_buf) {
+    rc = dev_alloc(c, &c->fft_buf, cplx * (dbl ? 16 : 8), "spectrum buffer");
+    if (rc) return rc;
+    c->fft_bytes = cplx * (dbl ? 16 : 8);
+  }
+  if (!c->plan_ok) {
+    cufftResult r = cufftPlan3d(&c->plan, nz, ny, nx, dbl ? CUFFT_D2Z : CUFFT_R2C);
+    if (r != CUFFT_SUCCESS) {
+      set_err("cufftPlan3d failed (%d)", (int)r);
+      return BGK_ERR_CUDA;
+    }
+    c->plan_ok = 1;
+    cufftSetStream(c->plan, c->st);
+  }
+  if (c->nbins_alloc < nbins) {
+    if (c->d_bins) {
+      cudaFree(c->d_bins);
+      c->dev_bytes -= (long long)c->nbins_alloc * 8;
+      c->d_bins = nullptr;
+    }
+    rc = dev_alloc(c, (void**)&c->d_bins, (size_t)nbins * 8, "spectrum bins");
+    if (rc) return rc;
+    c->nbins_alloc = nbins;
+  }
+  CK(cudaMemsetAsync(c->d_bins, 0, (size_t)nbins * 8, c->st));
+  const size_t n = (size_t)ncell(c);
+  const double norm = 1.0 / ((double)n * (double)n);
+  for (int d = 0; d < 3; ++d) {
+    cufftResult r = dbl ? cufftExecD2Z(c->plan, (double*)c->vel + d * n, (cufftDoubleComplex*)c->fft_buf)
+                        : cufftExecR2C(c->plan, (float*)c->vel + d * n, (cufftComplex*)c->fft_buf);
+    if (r != CUFFT_SUCCESS) {
+      set_err("cufftExec failed (%d)", (int)r);
+      return BGK_ERR_CUDA;
+    }
+    CK(launch_spectrum_bins(c->fft_buf, c->form, nx, ny, nz, nbins, c->d_bins, norm, c->st));
+    c->launches++;
+  }
+  CK(cudaMemcpyAsync(ek, c->d_bins, (size_t)nbins * 8, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return BGK_OK;
+}
+
+int bgk_get_scale(const bgk_ctx* c, double* s) {
+  if (!c || !s) return BGK_ERR_INVALID;
+  *s = c->scale;
+  return BGK_OK;
+}
+
+int bgk_get_omega(const bgk_ctx* c, double* o) {
+  if (!c || !o) return BGK_ERR_INVALID;
+  *o = c->omega;
+  return BGK_OK;
+}
+
+int bgk_get_step(const bgk_ctx* c, long long* s) {
+  if (!c || !s) return BGK_ERR_INVALID;
+  *s = c->step;
+  return BGK_OK;
+}
+
+int bgk_get_device_bytes(const bgk_ctx* c, long long* b) {
+  if (!c || !b) return BGK_ERR_INVALID;
+  *b = c->dev_bytes;
+  return BGK_OK;
+}
+
+int bgk_get_launch_count(const bgk_ctx* c, long long* n) {
+  if (!c || !n) return BGK_ERR_INVALID;
+  *n = c->launches;
+  return BGK_OK;
+}
+
+void* bgk_get_stream(const bgk_ctx* c) { return c ? (void*)c->st : nullptr; }
+
+int bgk_synchronize(bgk_ctx* c) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  CK(cudaSetDevice(c->p.device));
+  CK(cudaStreamSynchronize(c->st));
+  return BGK_OK;
+}
+
+int bgk_shift3(const void* in1, const void* in2, const void* in3, void* out1, void* out2, void* out3, int nx, int ny,
+               int nz, int elem_bytes, int reverse, void* stream) {
+  if (!in1 || !in2 || !in3 || !out1 || !out2 || !out3 || nx < 1 || ny < 1 || nz < 1 ||
+      (elem_bytes != 2 && elem_bytes != 4 && elem_bytes != 8)) {
+    set_err("bgk_shift3: invalid argument");
+    return BGK_ERR_INVALID;
+  }
+  const void* in[3] = {in1, in2, in3};
+  void* out[3] = {out1, out2, out3};
+  CK(launch_shift3(in, out, nx, ny, nz, elem_bytes, reverse, (cudaStream_t)stream));
+  return BGK_OK;
+}
+
+const char* bgk_strerror(int code) {
+  switch (code) {
+    case BGK_OK: return "ok";
+    case BGK_SKIPPED: return "not a diagnostic step";
+    case BGK_ERR_INVALID: return "invalid argument";
+    case BGK_ERR_CUDA: return "CUDA error";
+    case BGK_ERR_NOMEM: return "device memory allocation failed";
+    case BGK_ERR_STATE: return "call out of order";
+    case BGK_ERR_NONFINITE: return "non-finite density or velocity";
+  }
+  return "unknown error";
+}
+
+const char* bgk_last_error(void) { return g_err; }
+
+const char* bgk_version(void) { return "bgk3d-b200 0.1 (sm_100a)"; }
+
+}  // extern "C"

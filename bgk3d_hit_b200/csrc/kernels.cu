@@ -1,0 +1,675 @@
+// CUDA kernels of the BGK3D_HIT hot path for sm_100a.
+//
+//   k_two        fused pull-stream + BGK collide, two lattices, pop 19 in place
+//                (SRC/col_MC.F90:98-421); periodic wrap by index arithmetic
+//                replaces the halo exchange of SRC/bcond.comm.step3.F90
+//   k_aa         in-place AA-pattern variant of the same update (no reference
+//                counterpart; same per-cell arithmetic)
+//   k_init_*     equilibrium initial conditions (SRC/init.F90:83-141)
+//   k_diag       diagno + dissipation + strain-rate sums (SRC/diagno.F90:73-121,
+//                SRC/dissipation.F90:65-269) as deterministic compensated
+//                per-block partials
+//   k_enstrophy  0.5|curl u|^2 from the local velocity field
+//   k_shift3     shift-only stencil of SRC/do_somethingGPU.F90:37-100
+#include "kernels.h"
+
+namespace bgk {
+
+__device__ __forceinline__ int wrapi(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
+
+__device__ __forceinline__ double ldg(const double* p) { return __ldg(p); }
+__device__ __forceinline__ float ldg(const float* p) { return __ldg(p); }
+__device__ __forceinline__ __half ldg(const __half* p) { return __ldg(p); }
+
+// Moments of 19 local deviations in the reference's order
+// (SRC/diagno.F90:96-104, identical to SRC/col_MC.F90:133-141).
+template <class V>
+__device__ __forceinline__ V moments(const V (&x)[Q], V& vx, V& vy, V& vz) {
+  using N = Num<V>;
+  const V uno = N::c(1.0), cte1 = N::c(1.0);
+  V rho = x[0] + x[1] + x[2] + x[3] + x[4] + x[5] + x[6] + x[7]
+        + x[8] + x[9] + x[10] + x[11] + x[12] + x[13] + x[14] + x[15]
+        + x[16] + x[17] + x[18] + cte1;
+  V rhoinv = uno / rho;
+  vx = (x[0] + x[1] + x[2] + x[3] + x[4] - x[9] - x[10] - x[11] - x[12] - x[13]) * rhoinv;
+  vy = (x[2] + x[6] + x[7] + x[8] + x[11] - x[0] - x[9] - x[15] - x[16] - x[17]) * rhoinv;
+  vz = (x[3] + x[5] + x[6] + x[12] + x[17] - x[1] - x[8] - x[10] - x[14] - x[15]) * rhoinv;
+  return rho;
+}
+
+// Launch shape of the per-cell stream kernels: x-rows in blockDim.x.
+struct Shape { dim3 grid, block; };
+static Shape cell_shape(const Geo& g) {
+  int tx = g.nx >= 128 ? 128 : ((g.nx + 31) / 32) * 32;
+  int ty = 256 / tx;
+  Shape s;
+  s.block = dim3(tx, ty, 1);
+  s.grid = dim3((g.nx + tx - 1) / tx, (g.ny + ty - 1) / ty, g.nz);
+  return s;
+}
+
+static int grid_1d(long long n, int threads, int cap) {
+  long long b = (n + threads - 1) / threads;
+  return (int)(b < cap ? (b < 1 ? 1 : b) : cap);
+}
+
+// ------------------------------------------------------------- two lattice
+template <class F>
+__global__ void __launch_bounds__(256) k_two(Pops<const typename F::S> src, Pops<typename F::S> dst, Geo g,
+                                             typename F::R omega, typename F::R scale, typename F::R inv) {
+  using S = typename F::S; using V = typename F::V; using N = Num<V>;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  if (i >= g.nx || j >= g.ny) return;
+  const int im = i == 0 ? g.nx - 1 : i - 1, ip = i == g.nx - 1 ? 0 : i + 1;
+  const int jm = j == 0 ? g.ny - 1 : j - 1, jp = j == g.ny - 1 ? 0 : j + 1;
+  const int km = k == 0 ? g.nz - 1 : k - 1, kp = k == g.nz - 1 ? 0 : k + 1;
+  V x[Q];
+#pragma unroll
+  for (int q = 0; q < Q; ++q) {
+    // pull from (i - cx, j - cy, k - cz), SRC/col_MC.F90:113-131
+    const int ii = cxq(q) > 0 ? im : (cxq(q) < 0 ? ip : i);
+    const int jj = cyq(q) > 0 ? jm : (cyq(q) < 0 ? jp : j);
+    const int kk = czq(q) > 0 ? km : (czq(q) < 0 ? kp : k);
+    const int off = ii + g.sx * (jj + g.ny * kk);
+    const S s = (q == Q - 1) ? dst.p[Q - 1][off] : ldg(src.p[q] + off);
+    x[q] = N::wrap(F::dec(s, inv));
+  }
+  collide<V>(x, N::wrap(omega));
+  const int o = i + g.sx * (j + g.ny * k);
+#pragma unroll
+  for (int q = 0; q < Q; ++q) dst.p[q][o] = F::enc(N::raw(x[q]), scale);
+}
+
+// --------------------------------------------------------------- AA pattern
+// Even step: g_q(x) = slot q at x; result q -> slot opp(q) at x.
+// Odd step:  g_q(x) = slot opp(q) at x - c_q; result q -> slot q at x + c_q.
+// Each thread reads exactly the locations it writes, so the update is
+// race-free in place.
+template <class F, bool ODD>
+__global__ void __launch_bounds__(256) k_aa(Pops<typename F::S> a, Geo g, typename F::R omega,
+                                            typename F::R scale, typename F::R inv) {
+  using V = typename F::V; using N = Num<V>;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  if (i >= g.nx || j >= g.ny) return;
+  const int o = i + g.sx * (j + g.ny * k);
+  V x[Q];
+  int off[Q];
+  if (ODD) {
+    const int im = i == 0 ? g.nx - 1 : i - 1, ip = i == g.nx - 1 ? 0 : i + 1;
+    const int jm = j == 0 ? g.ny - 1 : j - 1, jp = j == g.ny - 1 ? 0 : j + 1;
+    const int km = k == 0 ? g.nz - 1 : k - 1, kp = k == g.nz - 1 ? 0 : k + 1;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      // location x - c_q (read, slot opp(q)) == location x + c_opp(q) (write, slot opp(q))
+      const int ii = cxq(q) > 0 ? im : (cxq(q) < 0 ? ip : i);
+      const int jj = cyq(q) > 0 ? jm : (cyq(q) < 0 ? jp : j);
+      const int kk = czq(q) > 0 ? km : (czq(q) < 0 ? kp : k);
+      off[q] = ii + g.sx * (jj + g.ny * kk);
+    }
+#pragma unroll
+    for (int q = 0; q < Q; ++q) x[q] = N::wrap(F::dec(a.p[oppq(q)][off[q]], inv));
+  } else {
+#pragma unroll
+    for (int q = 0; q < Q; ++q) x[q] = N::wrap(F::dec(a.p[q][o], inv));
+  }
+  collide<V>(x, N::wrap(omega));
+  if (ODD) {
+#pragma unroll
+    for (int q = 0; q < Q; ++q) a.p[q][off[oppq(q)]] = F::enc(N::raw(x[q]), scale);
+  } else {
+#pragma unroll
+    for (int q = 0; q < Q; ++q) a.p[oppq(q)][o] = F::enc(N::raw(x[q]), scale);
+  }
+}
+
+// ------------------------------------------------------ initial conditions
+// Per-cell equilibrium deviation of SRC/init.F90:97-137 (cte1 = 0):
+// out_q = crho*w_q*(0 + rf*(c.u) + qf*(3*(c.u)^2 - |u|^2)), with each linear
+// and quadratic term written as in the reference text.
+template <class V>
+__device__ __forceinline__ void eq_init(V xj, V yj, V zj, V crho, V (&out)[Q]) {
+  using N = Num<V>;
+  const V rf = N::c(3.0), qf = N::c(1.5), three = N::c(3.0), zero = N::c(0.0), cte1 = zero;
+  const V p0 = N::c(1.0 / 3.0), p1 = N::c(1.0 / 18.0), p2 = N::c(1.0 / (3.0 * 3.0 * (1.0 + 3.0)));
+  const V cvsq = xj * xj + yj * yj + zj * zj;
+  V cx[Q];
+  cx[0]  = rf * (xj - yj) + qf * (three * (xj - yj) * (xj - yj) - cvsq);
+  cx[1]  = rf * (xj - zj) + qf * (three * (xj - zj) * (xj - zj) - cvsq);
+  cx[2]  = rf * (xj + yj) + qf * (three * (xj + yj) * (xj + yj) - cvsq);
+  cx[3]  = rf * (xj + zj) + qf * (three * (xj + zj) * (xj + zj) - cvsq);
+  cx[4]  = rf * (xj) + qf * (three * (xj) * (xj) - cvsq);
+  cx[5]  = rf * (zj) + qf * (three * (zj) * (zj) - cvsq);
+  cx[6]  = rf * (yj + zj) + qf * (three * (yj + zj) * (yj + zj) - cvsq);
+  cx[7]  = rf * (yj) + qf * (three * (yj) * (yj) - cvsq);
+  cx[8]  = rf * (yj - zj) + qf * (three * (yj - zj) * (yj - zj) - cvsq);
+  cx[9]  = rf * (-xj - yj) + qf * (three * (xj + yj) * (xj + yj) - cvsq);
+  cx[10] = rf * (-xj - zj) + qf * (three * (xj + zj) * (xj + zj) - cvsq);
+  cx[11] = rf * (-xj + yj) + qf * (three * (xj - yj) * (xj - yj) - cvsq);
+  cx[12] = rf * (-xj + zj) + qf * (three * (xj - zj) * (xj - zj) - cvsq);
+  cx[13] = rf * (-xj) + qf * (three * (xj) * (xj) - cvsq);
+  cx[14] = rf * (-zj) + qf * (three * (zj) * (zj) - cvsq);
+  cx[15] = rf * (-yj - zj) + qf * (three * (yj + zj) * (yj + zj) - cvsq);
+  cx[16] = rf * (-yj) + qf * (three * (yj) * (yj) - cvsq);
+  cx[17] = rf * (-yj + zj) + qf * (three * (yj - zj) * (yj - zj) - cvsq);
+  cx[18] = rf * zero + qf * (three * zero * zero - cvsq);
+#pragma unroll
+  for (int q = 0; q < Q; ++q) {
+    const bool w1 = (q == 4 || q == 5 || q == 7 || q == 13 || q == 14 || q == 16);
+    const V w = q == 18 ? p0 : (w1 ? p1 : p2);
+    out[q] = crho * w * (cte1 + cx[q]);
+  }
+}
+
+__device__ __forceinline__ double dsin(double x) { return sin(x); }
+__device__ __forceinline__ double dcos(double x) { return cos(x); }
+__device__ __forceinline__ float dsin(float x) { return sinf(x); }
+__device__ __forceinline__ float dcos(float x) { return cosf(x); }
+
+template <class F>
+__device__ __forceinline__ void store_cell(Pops<typename F::S>& a, int lay, int o, typename F::V (&v)[Q],
+                                           typename F::R scale) {
+  using N = Num<typename F::V>;
+#pragma unroll
+  for (int q = 0; q < Q; ++q) a.p[lay == LAY_AAE ? oppq(q) : q][o] = F::enc(N::raw(v[q]), scale);
+}
+
+// Largest |deviation| of a cell, for choosing the FP16 scale.
+template <class V>
+__device__ __forceinline__ float cell_maxabs(const V (&v)[Q]) {
+  float m = 0.f;
+#pragma unroll
+  for (int q = 0; q < Q; ++q) m = fmaxf(m, fabsf((float)Num<V>::raw(v[q])));
+  return m;
+}
+
+// Taylor-Green vortex, SRC/init.F90:83-141 (offsets zero, one box).
+// maxbits != nullptr: measure max |deviation| only (atomicMax on the bits of a
+// non-negative float), store nothing.
+template <class F>
+__global__ void k_init_tgv(Pops<typename F::S> a, Geo g, int lay, typename F::R u0r, int faithful,
+                           typename F::R scale, unsigned int* maxbits) {
+  using R = typename F::R; using V = typename F::V; using N = Num<V>;
+  const long long n = (long long)g.nx * g.ny * g.nz;
+  float tmax = 0.f;
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(c % g.nx), j = (int)((c / g.nx) % g.ny), k = (int)(c / ((long long)g.nx * g.ny));
+    // reference interior indices are 1-based
+    const int ir = i + 1, jr = j + 1, kr = k + 1;
+    R x, y, z, pi;
+    if (faithful) {
+      x = (R)(((float)ir - 0.5f) / (float)g.nx);
+      y = (R)(((float)jr - 0.5f) / (float)g.ny);
+      z = (R)(((float)kr - 0.5f) / (float)g.nz);
+      pi = (R)3.141592653589793238462643383279f;
+    } else {
+      x = (R)(((double)ir - 0.5) / (double)g.nx);
+      y = (R)(((double)jr - 0.5) / (double)g.ny);
+      z = (R)(((double)kr - 0.5) / (double)g.nz);
+      pi = (R)3.141592653589793238462643383279;
+    }
+    const V two = N::c(2.0), four = N::c(4.0), u0 = N::wrap(u0r), P = N::wrap(pi);
+    const V X = N::wrap(x), Y = N::wrap(y), Z = N::wrap(z);
+    const R ax = N::raw(two * P * X), ay = N::raw(two * P * Y), az = N::raw(two * P * Z);
+    const V xj = u0 * N::wrap(dsin(ax)) * N::wrap(dcos(ay)) * N::wrap(dcos(az));
+    const V yj = -(u0 * N::wrap(dcos(ax)) * N::wrap(dsin(ay)) * N::wrap(dcos(az)));
+    const V zj = N::c(0.0);
+    V crho = N::c(1.0);
+    if (faithful) {
+      const R bx = N::raw(four * P * X), by = N::raw(four * P * Y), bz = N::raw(four * P * Z);
+      crho = N::c(1.0) + ((u0 * u0) / (N::c(16.0) * N::c(3.0))) * (N::wrap(dcos(bx)) + N::wrap(dcos(by))) *
+                             (N::wrap(dcos(bz)) + N::c(2.0));
+    }
+    V out[Q];
+    eq_init<V>(xj, yj, zj, crho, out);
+    if (maxbits) tmax = fmaxf(tmax, cell_maxabs<V>(out));
+    else store_cell<F>(a, lay, i + g.sx * (j + g.ny * k), out, scale);
+  }
+  if (maxbits) atomicMax(maxbits, __float_as_uint(tmax));
+}
+
+// Equilibrium from a staged velocity slab (planes k0 .. k0+nk-1, dense
+// Fortran order) at uniform density rho.
+template <class F>
+__global__ void k_init_vel(Pops<typename F::S> a, Geo g, int lay, const double* __restrict__ u,
+                           const double* __restrict__ v, const double* __restrict__ w, double rho, int k0, int nk,
+                           typename F::R scale, unsigned int* maxbits) {
+  using R = typename F::R; using V = typename F::V; using N = Num<V>;
+  const long long n = (long long)g.nx * g.ny * nk;
+  float tmax = 0.f;
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(c % g.nx), j = (int)((c / g.nx) % g.ny), k = k0 + (int)(c / ((long long)g.nx * g.ny));
+    V out[Q];
+    eq_init<V>(N::wrap((R)u[c]), N::wrap((R)v[c]), N::wrap((R)w[c]), N::wrap((R)rho), out);
+    if (maxbits) tmax = fmaxf(tmax, cell_maxabs<V>(out));
+    else store_cell<F>(a, lay, i + g.sx * (j + g.ny * k), out, scale);
+  }
+  if (maxbits) atomicMax(maxbits, __float_as_uint(tmax));
+}
+
+// ------------------------------------------------------- reference access
+// Location of the reference's a_q at cell (i,j,k) + d for a given layout.
+template <int LAY>
+__device__ __forceinline__ int ref_slot(int q) { return LAY == LAY_AAE ? oppq(q) : q; }
+template <int LAY>
+__device__ __forceinline__ int ref_off(const Geo& g, int q, int i, int j, int k, int dx, int dy, int dz) {
+  if (LAY == LAY_AAN) { dx += cxq(q); dy += cyq(q); dz += czq(q); }
+  return wrapi(i + dx, g.nx) + g.sx * (wrapi(j + dy, g.ny) + g.ny * wrapi(k + dz, g.nz));
+}
+
+template <class F, int LAY>
+__global__ void k_export(Pops<const typename F::S> a, Geo g, int q, typename F::S* out_s, double* out_d,
+                         typename F::R inv) {
+  const long long n = (long long)g.nx * g.ny * g.nz;
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(c % g.nx), j = (int)((c / g.nx) % g.ny), k = (int)(c / ((long long)g.nx * g.ny));
+    const typename F::S s = a.p[ref_slot<LAY>(q)][ref_off<LAY>(g, q, i, j, k, 0, 0, 0)];
+    if (out_s) out_s[c] = s;
+    if (out_d) out_d[c] = (double)F::dec(s, inv);
+  }
+}
+
+template <class F, int LAY>
+__global__ void k_import(Pops<typename F::S> a, Geo g, int q, const typename F::S* __restrict__ in) {
+  const long long n = (long long)g.nx * g.ny * g.nz;
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(c % g.nx), j = (int)((c / g.nx) % g.ny), k = (int)(c / ((long long)g.nx * g.ny));
+    a.p[ref_slot<LAY>(q)][ref_off<LAY>(g, q, i, j, k, 0, 0, 0)] = in[c];
+  }
+}
+
+// ------------------------------------------------------------ diagnostics
+struct KS { double s, c; };
+// Neumaier step; explicit _rn operations keep it free of FMA contraction.
+__device__ __forceinline__ void kadd(KS& a, double v) {
+  const double t = __dadd_rn(a.s, v);
+  if (fabs(a.s) >= fabs(v)) a.c = __dadd_rn(a.c, __dadd_rn(__dsub_rn(a.s, t), v));
+  else a.c = __dadd_rn(a.c, __dadd_rn(__dsub_rn(v, t), a.s));
+  a.s = t;
+}
+__device__ __forceinline__ void kcomb(KS& a, const KS& b) {
+  kadd(a, b.s);
+  a.c = __dadd_rn(a.c, b.c);
+}
+
+// Fixed-order block reduction of one quantity; thread 0 returns the result.
+__device__ __forceinline__ KS block_reduce(KS v, KS* sh) {
+  const int t = threadIdx.x;
+  sh[t] = v;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (t < s) { KS a = sh[t]; kcomb(a, sh[t + s]); sh[t] = a; }
+    __syncthreads();
+  }
+  KS r = sh[0];
+  __syncthreads();
+  return r;
+}
+
+// Quantities: 0 rho, 1 ux, 2 uy, 3 uz, 4 0.5|u|^2 (local populations,
+// SRC/diagno.F90:96-111); 5 0.5|u|^2, 6 2*svisc*Ptotal (pulled populations,
+// SRC/dissipation.F90:76-249); 7 2*nu*S:S with S = -3*omega*Pi/(2*rho);
+// 8 non-finite cell count; 9 enstrophy (k_enstrophy).
+template <class F, int LAY>
+__global__ void __launch_bounds__(DIAG_THREADS) k_diag(Pops<const typename F::S> a, Geo g, double svisc,
+                                                       double omega, typename F::R inv, double* partials,
+                                                       typename F::R* vel) {
+  using R = typename F::R; using V = typename F::V; using N = Num<V>;
+  __shared__ KS sh[DIAG_THREADS];
+  KS acc[ND];
+#pragma unroll
+  for (int d = 0; d < ND; ++d) acc[d] = {0.0, 0.0};
+  const long long n = (long long)g.nx * g.ny * g.nz;
+  const V svr = N::wrap((R)svisc);
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(c % g.nx), j = (int)((c / g.nx) % g.ny), k = (int)(c / ((long long)g.nx * g.ny));
+    V x[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q)
+      x[q] = N::wrap(F::dec(a.p[ref_slot<LAY>(q)][ref_off<LAY>(g, q, i, j, k, 0, 0, 0)], inv));
+    V ux, uy, uz;
+    const V rho = moments<V>(x, ux, uy, uz);
+    const V ke = N::c(0.5) * (ux * ux + uy * uy + uz * uz);
+    kadd(acc[0], (double)N::raw(rho));
+    kadd(acc[1], (double)N::raw(ux));
+    kadd(acc[2], (double)N::raw(uy));
+    kadd(acc[3], (double)N::raw(uz));
+    kadd(acc[4], (double)N::raw(ke));
+    if (!isfinite(N::raw(rho)) || !isfinite(N::raw(ux)) || !isfinite(N::raw(uy)) || !isfinite(N::raw(uz)))
+      acc[8].s = __dadd_rn(acc[8].s, 1.0);
+    if (vel) { vel[c] = N::raw(ux); vel[n + c] = N::raw(uy); vel[2 * n + c] = N::raw(uz); }
+#pragma unroll
+    for (int q = 0; q < Q; ++q)
+      x[q] = N::wrap(F::dec(a.p[ref_slot<LAY>(q)][ref_off<LAY>(g, q, i, j, k, -cxq(q), -cyq(q), -czq(q))], inv));
+    V e[Q], vx, vy, vz;
+    const V rp = equilibrium<V>(x, e, vx, vy, vz);
+    const V vsq = vx * vx + vy * vy + vz * vz;
+    const V P = ptotal<V>(x, e);
+    kadd(acc[5], (double)N::raw(N::c(0.5) * vsq));
+    kadd(acc[6], (double)N::raw(N::c(2.0) * svr * P));
+    const double r = (double)N::raw(rp);
+    const double eps = __dmul_rn(__dmul_rn(__dmul_rn(2.0, svisc), __ddiv_rn(__dmul_rn(__dmul_rn(9.0, omega), omega),
+                                                                          __dmul_rn(__dmul_rn(4.0, r), r))),
+                                 (double)N::raw(P));
+    kadd(acc[7], eps);
+  }
+#pragma unroll
+  for (int d = 0; d < ND; ++d) {
+    const KS r = block_reduce(acc[d], sh);
+    if (threadIdx.x == 0) {
+      partials[(blockIdx.x * ND + d) * 2 + 0] = r.s;
+      partials[(blockIdx.x * ND + d) * 2 + 1] = r.c;
+    }
+  }
+}
+
+template <class R>
+__global__ void __launch_bounds__(DIAG_THREADS) k_enstrophy(const R* __restrict__ vel, int nx, int ny, int nz,
+                                                            double* partials) {
+  __shared__ KS sh[DIAG_THREADS];
+  KS acc = {0.0, 0.0};
+  const long long n = (long long)nx * ny * nz;
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(c % nx), j = (int)((c / nx) % ny), k = (int)(c / ((long long)nx * ny));
+    const int ip = i + 1 == nx ? 0 : i + 1, im = i == 0 ? nx - 1 : i - 1;
+    const int jp = j + 1 == ny ? 0 : j + 1, jm = j == 0 ? ny - 1 : j - 1;
+    const int kp = k + 1 == nz ? 0 : k + 1, km = k == 0 ? nz - 1 : k - 1;
+    auto U = [&](int comp, int a, int b, int d) -> double {
+      return (double)vel[comp * n + a + (long long)nx * (b + (long long)ny * d)];
+    };
+    using E = Ex<double>;
+    const E h = {0.5};
+    const E dwdy = h * (E{U(2, i, jp, k)} - E{U(2, i, jm, k)});
+    const E dvdz = h * (E{U(1, i, j, kp)} - E{U(1, i, j, km)});
+    const E dudz = h * (E{U(0, i, j, kp)} - E{U(0, i, j, km)});
+    const E dwdx = h * (E{U(2, ip, j, k)} - E{U(2, im, j, k)});
+    const E dvdx = h * (E{U(1, ip, j, k)} - E{U(1, im, j, k)});
+    const E dudy = h * (E{U(0, i, jp, k)} - E{U(0, i, jm, k)});
+    const E wx = dwdy - dvdz, wy = dudz - dwdx, wz = dvdx - dudy;
+    kadd(acc, (h * (wx * wx + wy * wy + wz * wz)).v);
+  }
+  const KS r = block_reduce(acc, sh);
+  if (threadIdx.x == 0) {
+    partials[(blockIdx.x * ND + 9) * 2 + 0] = r.s;
+    partials[(blockIdx.x * ND + 9) * 2 + 1] = r.c;
+  }
+}
+
+__global__ void __launch_bounds__(DIAG_THREADS) k_finalize(const double* __restrict__ partials, double* totals) {
+  __shared__ KS sh[DIAG_THREADS];
+  for (int d = 0; d < ND; ++d) {
+    KS acc = {0.0, 0.0};
+    for (int b = threadIdx.x; b < DIAG_BLOCKS; b += blockDim.x)
+      kcomb(acc, KS{partials[(b * ND + d) * 2], partials[(b * ND + d) * 2 + 1]});
+    const KS r = block_reduce(acc, sh);
+    if (threadIdx.x == 0) totals[d] = __dadd_rn(r.s, r.c);
+  }
+}
+
+template <class F, int LAY>
+__global__ void k_last_zj(Pops<const typename F::S> a, Geo g, typename F::R inv, double* out) {
+  using V = typename F::V; using N = Num<V>;
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  V x[Q];
+  for (int q = 0; q < Q; ++q)
+    x[q] = N::wrap(F::dec(a.p[ref_slot<LAY>(q)][ref_off<LAY>(g, q, g.nx - 1, g.ny - 1, g.nz - 1, 0, 0, 0)], inv));
+  V ux, uy, uz;
+  (void)moments<V>(x, ux, uy, uz);
+  *out = (double)N::raw(uz);
+}
+
+// --------------------------------------------------------------- spectrum
+template <class C>
+__global__ void k_spec_bins(const C* __restrict__ f, int nx, int ny, int nz, int nbins, double* bins, double norm) {
+  const int nxh = nx / 2 + 1;
+  const long long n = (long long)nxh * ny * nz;
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+    const int ix = (int)(c % nxh), iy = (int)((c / nxh) % ny), iz = (int)(c / ((long long)nxh * ny));
+    const int ky = iy <= ny / 2 ? iy : iy - ny, kz = iz <= nz / 2 ? iz : iz - nz;
+    // modes 0 < kx < nx/2 stand for their conjugate partner as well
+    const double w = (ix == 0 || (nx % 2 == 0 && ix == nx / 2)) ? 1.0 : 2.0;
+    const double kk = sqrt((double)ix * ix + (double)ky * ky + (double)kz * kz);
+    const int b = (int)floor(kk + 0.5);
+    if (b < nbins) {
+      const double re = (double)f[c].x, im = (double)f[c].y;
+      atomicAdd(bins + b, w * 0.5 * (re * re + im * im) * norm);
+    }
+  }
+}
+
+cudaError_t launch_spectrum_bins(const void* fft_out, int form, int nx, int ny, int nz, int nbins, double* bins,
+                                 double norm, cudaStream_t st) {
+  const long long n = (long long)(nx / 2 + 1) * ny * nz;
+  const int grid = grid_1d(n, 256, 148 * 16);
+  if (form == FORM_F64)
+    k_spec_bins<double2><<<grid, 256, 0, st>>>((const double2*)fft_out, nx, ny, nz, nbins, bins, norm);
+  else
+    k_spec_bins<float2><<<grid, 256, 0, st>>>((const float2*)fft_out, nx, ny, nz, nbins, bins, norm);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------- shift3
+template <class T>
+__global__ void k_shift3(const T* __restrict__ i1, const T* __restrict__ i2, const T* __restrict__ i3, T* o1, T* o2,
+                         T* o3, int nx, int ny, int nz, int dir) {
+  const long long n = (long long)nx * ny * nz;
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(c % nx), j = (int)((c / nx) % ny), k = (int)(c / ((long long)nx * ny));
+    const long long rowj = (long long)nx * (j + (long long)ny * k);
+    const int is = wrapi(i - dir, nx), js = wrapi(j - dir, ny), ks = wrapi(k - dir, nz);
+    o1[c] = __ldg(i1 + rowj + is);
+    o2[c] = __ldg(i2 + i + (long long)nx * (js + (long long)ny * k));
+    o3[c] = __ldg(i3 + i + (long long)nx * (j + (long long)ny * ks));
+  }
+}
+
+// ============================================================== launchers
+template <class S> static Pops<S> pops_of(const Lattice& L) {
+  Pops<S> p;
+  for (int q = 0; q < Q; ++q) p.p[q] = (S*)L.p[q];
+  return p;
+}
+
+template <class F>
+static cudaError_t two_impl(const Lattice& s, const Lattice& d, double omega, double scale, cudaStream_t st) {
+  using S = typename F::S; using R = typename F::R;
+  Pops<const S> ps = pops_of<const S>(s);
+  Pops<S> pd = pops_of<S>(d);
+  pd.p[Q - 1] = (S*)s.p[Q - 1];  // pop 19 in place (SRC/col_MC.F90:351)
+  Shape sh = cell_shape(s.g);
+  k_two<F><<<sh.grid, sh.block, 0, st>>>(ps, pd, s.g, (R)omega, (R)scale, (R)(1.0 / scale));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_two_lattice(const Lattice& src, const Lattice& dst, double omega, double scale, int variant,
+                               cudaStream_t st) {
+  (void)variant;
+  switch (src.form) {
+    case FORM_F64: return two_impl<F64>(src, dst, omega, scale, st);
+    case FORM_F32: return two_impl<F32>(src, dst, omega, scale, st);
+    case FORM_F16: return two_impl<F16>(src, dst, omega, scale, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+template <class F>
+static cudaError_t aa_impl(const Lattice& a, int odd, double omega, double scale, cudaStream_t st) {
+  using S = typename F::S; using R = typename F::R;
+  Shape sh = cell_shape(a.g);
+  if (odd) k_aa<F, true><<<sh.grid, sh.block, 0, st>>>(pops_of<S>(a), a.g, (R)omega, (R)scale, (R)(1.0 / scale));
+  else k_aa<F, false><<<sh.grid, sh.block, 0, st>>>(pops_of<S>(a), a.g, (R)omega, (R)scale, (R)(1.0 / scale));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_aa(const Lattice& a, int odd, double omega, double scale, cudaStream_t st) {
+  switch (a.form) {
+    case FORM_F64: return aa_impl<F64>(a, odd, omega, scale, st);
+    case FORM_F32: return aa_impl<F32>(a, odd, omega, scale, st);
+    case FORM_F16: return aa_impl<F16>(a, odd, omega, scale, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+template <class F>
+static cudaError_t tgv_impl(const Lattice& a, int lay, double u0, int faithful, double scale, unsigned int* mx,
+                            cudaStream_t st) {
+  using S = typename F::S; using R = typename F::R;
+  const long long n = (long long)a.g.nx * a.g.ny * a.g.nz;
+  k_init_tgv<F><<<grid_1d(n, 256, 148 * 32), 256, 0, st>>>(pops_of<S>(a), a.g, lay, (R)u0, faithful, (R)scale, mx);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_init_tgv(const Lattice& a, int lay, double u0, int faithful, double scale, unsigned int* mx,
+                            cudaStream_t st) {
+  switch (a.form) {
+    case FORM_F64: return tgv_impl<F64>(a, lay, u0, faithful, scale, mx, st);
+    case FORM_F32: return tgv_impl<F32>(a, lay, u0, faithful, scale, mx, st);
+    case FORM_F16: return tgv_impl<F16>(a, lay, u0, faithful, scale, mx, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+template <class F>
+static cudaError_t vel_impl(const Lattice& a, int lay, const double* u, const double* v, const double* w, double rho,
+                            int k0, int nk, double scale, unsigned int* mx, cudaStream_t st) {
+  using S = typename F::S; using R = typename F::R;
+  const long long n = (long long)a.g.nx * a.g.ny * nk;
+  k_init_vel<F><<<grid_1d(n, 256, 148 * 32), 256, 0, st>>>(pops_of<S>(a), a.g, lay, u, v, w, rho, k0, nk, (R)scale,
+                                                           mx);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_init_velocity(const Lattice& a, int lay, const double* u, const double* v, const double* w,
+                                 double rho, int k0, int nk, double scale, unsigned int* mx, cudaStream_t st) {
+  switch (a.form) {
+    case FORM_F64: return vel_impl<F64>(a, lay, u, v, w, rho, k0, nk, scale, mx, st);
+    case FORM_F32: return vel_impl<F32>(a, lay, u, v, w, rho, k0, nk, scale, mx, st);
+    case FORM_F16: return vel_impl<F16>(a, lay, u, v, w, rho, k0, nk, scale, mx, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+template <class F, int LAY>
+static void export_lay(const Lattice& a, int q, void* ds, double* dd, double scale, cudaStream_t st) {
+  using S = typename F::S; using R = typename F::R;
+  const long long n = (long long)a.g.nx * a.g.ny * a.g.nz;
+  k_export<F, LAY><<<grid_1d(n, 256, 148 * 32), 256, 0, st>>>(pops_of<const S>(a), a.g, q, (S*)ds, dd,
+                                                               (R)(1.0 / scale));
+}
+template <class F>
+static cudaError_t export_impl(const Lattice& a, int lay, int q, void* ds, double* dd, double scale, cudaStream_t st) {
+  if (lay == LAY_TWO) export_lay<F, LAY_TWO>(a, q, ds, dd, scale, st);
+  else if (lay == LAY_AAE) export_lay<F, LAY_AAE>(a, q, ds, dd, scale, st);
+  else export_lay<F, LAY_AAN>(a, q, ds, dd, scale, st);
+  return cudaGetLastError();
+}
+cudaError_t launch_export(const Lattice& a, int lay, int q, void* ds, double* dd, double scale, cudaStream_t st) {
+  switch (a.form) {
+    case FORM_F64: return export_impl<F64>(a, lay, q, ds, dd, scale, st);
+    case FORM_F32: return export_impl<F32>(a, lay, q, ds, dd, scale, st);
+    case FORM_F16: return export_impl<F16>(a, lay, q, ds, dd, scale, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+template <class F, int LAY>
+static void import_lay(const Lattice& a, int q, const void* ds, cudaStream_t st) {
+  using S = typename F::S;
+  const long long n = (long long)a.g.nx * a.g.ny * a.g.nz;
+  k_import<F, LAY><<<grid_1d(n, 256, 148 * 32), 256, 0, st>>>(pops_of<S>(a), a.g, q, (const S*)ds);
+}
+template <class F>
+static cudaError_t import_impl(const Lattice& a, int lay, int q, const void* ds, cudaStream_t st) {
+  if (lay == LAY_TWO) import_lay<F, LAY_TWO>(a, q, ds, st);
+  else if (lay == LAY_AAE) import_lay<F, LAY_AAE>(a, q, ds, st);
+  else import_lay<F, LAY_AAN>(a, q, ds, st);
+  return cudaGetLastError();
+}
+cudaError_t launch_import(const Lattice& a, int lay, int q, const void* ds, cudaStream_t st) {
+  switch (a.form) {
+    case FORM_F64: return import_impl<F64>(a, lay, q, ds, st);
+    case FORM_F32: return import_impl<F32>(a, lay, q, ds, st);
+    case FORM_F16: return import_impl<F16>(a, lay, q, ds, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+template <class F, int LAY>
+static void diag_lay(const Lattice& a, double svisc, double omega, double scale, double* partials, void* vel,
+                     cudaStream_t st) {
+  using S = typename F::S; using R = typename F::R;
+  k_diag<F, LAY><<<DIAG_BLOCKS, DIAG_THREADS, 0, st>>>(pops_of<const S>(a), a.g, svisc, omega, (R)(1.0 / scale),
+                                                       partials, (R*)vel);
+}
+template <class F>
+static cudaError_t diag_impl(const Lattice& a, int lay, double svisc, double omega, double scale, double* partials,
+                             void* vel, cudaStream_t st) {
+  if (lay == LAY_TWO) diag_lay<F, LAY_TWO>(a, svisc, omega, scale, partials, vel, st);
+  else if (lay == LAY_AAE) diag_lay<F, LAY_AAE>(a, svisc, omega, scale, partials, vel, st);
+  else diag_lay<F, LAY_AAN>(a, svisc, omega, scale, partials, vel, st);
+  return cudaGetLastError();
+}
+cudaError_t launch_diag(const Lattice& a, int lay, double svisc, double omega, double scale, double* partials,
+                        void* vel, cudaStream_t st) {
+  switch (a.form) {
+    case FORM_F64: return diag_impl<F64>(a, lay, svisc, omega, scale, partials, vel, st);
+    case FORM_F32: return diag_impl<F32>(a, lay, svisc, omega, scale, partials, vel, st);
+    case FORM_F16: return diag_impl<F16>(a, lay, svisc, omega, scale, partials, vel, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_enstrophy(const Lattice& a, const void* vel, double* partials, cudaStream_t st) {
+  if (a.form == FORM_F64)
+    k_enstrophy<double><<<DIAG_BLOCKS, DIAG_THREADS, 0, st>>>((const double*)vel, a.g.nx, a.g.ny, a.g.nz, partials);
+  else
+    k_enstrophy<float><<<DIAG_BLOCKS, DIAG_THREADS, 0, st>>>((const float*)vel, a.g.nx, a.g.ny, a.g.nz, partials);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_finalize(const double* partials, double* totals, cudaStream_t st) {
+  k_finalize<<<1, DIAG_THREADS, 0, st>>>(partials, totals);
+  return cudaGetLastError();
+}
+
+template <class F>
+static cudaError_t lastzj_impl(const Lattice& a, int lay, double scale, double* out, cudaStream_t st) {
+  using S = typename F::S; using R = typename F::R;
+  const R inv = (R)(1.0 / scale);
+  if (lay == LAY_TWO) k_last_zj<F, LAY_TWO><<<1, 32, 0, st>>>(pops_of<const S>(a), a.g, inv, out);
+  else if (lay == LAY_AAE) k_last_zj<F, LAY_AAE><<<1, 32, 0, st>>>(pops_of<const S>(a), a.g, inv, out);
+  else k_last_zj<F, LAY_AAN><<<1, 32, 0, st>>>(pops_of<const S>(a), a.g, inv, out);
+  return cudaGetLastError();
+}
+cudaError_t launch_last_zj(const Lattice& a, int lay, double scale, double* out, cudaStream_t st) {
+  switch (a.form) {
+    case FORM_F64: return lastzj_impl<F64>(a, lay, scale, out, st);
+    case FORM_F32: return lastzj_impl<F32>(a, lay, scale, out, st);
+    case FORM_F16: return lastzj_impl<F16>(a, lay, scale, out, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_shift3(const void* const in[3], void* const out[3], int nx, int ny, int nz, int elem_bytes,
+                          int reverse, cudaStream_t st) {
+  const long long n = (long long)nx * ny * nz;
+  const int grid = grid_1d(n, 256, 148 * 16);
+  const int dir = reverse ? -1 : 1;
+  if (elem_bytes == 8)
+    k_shift3<double><<<grid, 256, 0, st>>>((const double*)in[0], (const double*)in[1], (const double*)in[2],
+                                           (double*)out[0], (double*)out[1], (double*)out[2], nx, ny, nz, dir);
+  else if (elem_bytes == 4)
+    k_shift3<float><<<grid, 256, 0, st>>>((const float*)in[0], (const float*)in[1], (const float*)in[2],
+                                          (float*)out[0], (float*)out[1], (float*)out[2], nx, ny, nz, dir);
+  else if (elem_bytes == 2)
+    k_shift3<__half><<<grid, 256, 0, st>>>((const __half*)in[0], (const __half*)in[1], (const __half*)in[2],
+                                           (__half*)out[0], (__half*)out[1], (__half*)out[2], nx, ny, nz, dir);
+  else
+    return cudaErrorInvalidValue;
+  return cudaGetLastError();
+}
+
+}  // namespace bgk

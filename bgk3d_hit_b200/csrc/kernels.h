@@ -1,0 +1,66 @@
+// Host-side launchers of the library's kernels (internal interface between
+// the C-ABI layer and the kernels; not exported).
+#pragma once
+#include <cuda_runtime.h>
+#include "lattice.cuh"
+
+namespace bgk {
+
+enum Form { FORM_F64 = 0, FORM_F32 = 1, FORM_F16 = 2 };
+// How the reference's a_q(x) (post-collision, not yet streamed) is stored:
+//   LAY_TWO : two-lattice, slot q at x
+//   LAY_AAE : AA pattern after an even step / after init, slot opp(q) at x
+//   LAY_AAN : AA pattern after an odd step, slot q at x + c_q
+enum Layout { LAY_TWO = 0, LAY_AAE = 1, LAY_AAN = 2 };
+
+struct Lattice {
+  int form;
+  Geo g;
+  void* p[Q];  // population base pointers
+};
+
+// Number of accumulated diagnostic quantities (see kernels.cu).
+constexpr int ND = 10;
+constexpr int DIAG_BLOCKS = 148 * 4;
+constexpr int DIAG_THREADS = 256;
+
+// Two-lattice fused pull-stream + collide: src -> dst (pops 1..18), pop 19 in
+// place in src.
+cudaError_t launch_two_lattice(const Lattice& src, const Lattice& dst, double omega, double scale, int variant,
+                               cudaStream_t st);
+// AA pattern: even (local read, reversed local write) or odd (pull from
+// neighbours' opposite slots, push to neighbours).
+cudaError_t launch_aa(const Lattice& a, int odd, double omega, double scale, cudaStream_t st);
+
+// Initial conditions (write layout `lay`, which must be LAY_TWO or LAY_AAE).
+// mx != nullptr: only measure max |f - w| into *mx (bits of a float), no store.
+cudaError_t launch_init_tgv(const Lattice& a, int lay, double u0, int faithful, double scale, unsigned int* mx,
+                            cudaStream_t st);
+cudaError_t launch_init_velocity(const Lattice& a, int lay, const double* u, const double* v, const double* w,
+                                 double rho, int k0, int nk, double scale, unsigned int* mx, cudaStream_t st);
+
+// Population q in reference semantics, dense Fortran order.
+cudaError_t launch_export(const Lattice& a, int lay, int q, void* dense_stored, double* dense_dev, double scale,
+                          cudaStream_t st);
+cudaError_t launch_import(const Lattice& a, int lay, int q, const void* dense_stored, cudaStream_t st);
+
+// Diagnostics: per-block partial sums (Neumaier pairs) of ND quantities.
+// vel (optional, 3*N values of the arithmetic type) receives the local velocity.
+cudaError_t launch_diag(const Lattice& a, int lay, double svisc, double omega, double scale, double* partials,
+                        void* vel, cudaStream_t st);
+cudaError_t launch_enstrophy(const Lattice& a, const void* vel, double* partials, cudaStream_t st);
+// Sums DIAG_BLOCKS partials into ND totals (fixed order, compensated).
+cudaError_t launch_finalize(const double* partials, double* totals, cudaStream_t st);
+// Faithful-mode helper: zj of the last cell (i=l, j=m, k=n) into *out.
+cudaError_t launch_last_zj(const Lattice& a, int lay, double scale, double* out, cudaStream_t st);
+
+// Shell binning of one transformed velocity component (nz x ny x (nx/2+1)
+// complex values of the arithmetic type): bins[round(|k|)] += w*0.5|u_hat|^2*norm.
+cudaError_t launch_spectrum_bins(const void* fft_out, int form, int nx, int ny, int nz, int nbins, double* bins,
+                                 double norm, cudaStream_t st);
+
+// Streaming-only calibrator (shift of three scalar fields by one cell).
+cudaError_t launch_shift3(const void* const in[3], void* const out[3], int nx, int ny, int nz, int elem_bytes,
+                          int reverse, cudaStream_t st);
+
+}  // namespace bgk

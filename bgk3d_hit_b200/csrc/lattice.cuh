@@ -1,0 +1,188 @@
+// D3Q19 lattice, storage forms and the per-cell BGK collision shared by every
+// kernel of the library.
+//
+// Velocity set and pull offsets: SRC/alloca.F90:57-175, SRC/col_MC.F90:113-131
+// (population q of the reference is index q-1 here). Collision arithmetic:
+// SRC/col_MC.F90:133-219,333-351 in the deviation form (cte1 = 1, cte0 = 0).
+#pragma once
+#include <cuda_fp16.h>
+#include <cstdint>
+
+namespace bgk {
+
+constexpr int Q = 19;
+
+// c_q of the reference velocity set, q = 1..19 -> index 0..18.
+__host__ __device__ constexpr int cxq(int q) {
+  return q < 5 ? 1 : (q < 9 ? 0 : (q < 14 ? -1 : 0));
+}
+__host__ __device__ constexpr int cyq(int q) {
+  // -1 0 1 0 0 0 1 1 1 -1 0 1 0 0 0 -1 -1 -1 0
+  return (q == 0 || q == 9 || q == 15 || q == 16 || q == 17) ? -1
+         : (q == 2 || q == 6 || q == 7 || q == 8 || q == 11) ? 1 : 0;
+}
+__host__ __device__ constexpr int czq(int q) {
+  // 0 -1 0 1 0 1 1 0 -1 0 -1 0 1 0 -1 -1 0 1 0
+  return (q == 1 || q == 8 || q == 10 || q == 14 || q == 15) ? -1
+         : (q == 3 || q == 5 || q == 6 || q == 12 || q == 17) ? 1 : 0;
+}
+// Opposite direction, c(opp q) = -c(q). Pairs in the reference's 1-based
+// numbering: 1<->12, 2<->13, 3<->10, 4<->11, 5<->14, 6<->15, 7<->16, 8<->17,
+// 9<->18, 19 fixed.
+__host__ __device__ constexpr int oppq(int q) {
+  return q == 18 ? 18 : (q < 9 ? (q == 0 ? 11 : q == 1 ? 12 : q == 2 ? 9 : q == 3 ? 10 : q == 4 ? 13 : q + 9)
+                                  : (q == 9 ? 2 : q == 10 ? 3 : q == 11 ? 0 : q == 12 ? 1 : q == 13 ? 4 : q - 9));
+}
+
+// ---------------------------------------------------------------- arithmetic
+// Ex<T> rounds every operation separately (no FMA contraction), so device
+// results equal a host build that evaluates the same expressions in order.
+template <class T> struct Ex { T v; };
+__device__ __forceinline__ Ex<double> operator+(Ex<double> a, Ex<double> b) { return {__dadd_rn(a.v, b.v)}; }
+__device__ __forceinline__ Ex<double> operator-(Ex<double> a, Ex<double> b) { return {__dsub_rn(a.v, b.v)}; }
+__device__ __forceinline__ Ex<double> operator*(Ex<double> a, Ex<double> b) { return {__dmul_rn(a.v, b.v)}; }
+__device__ __forceinline__ Ex<double> operator/(Ex<double> a, Ex<double> b) { return {__ddiv_rn(a.v, b.v)}; }
+__device__ __forceinline__ Ex<float> operator+(Ex<float> a, Ex<float> b) { return {__fadd_rn(a.v, b.v)}; }
+__device__ __forceinline__ Ex<float> operator-(Ex<float> a, Ex<float> b) { return {__fsub_rn(a.v, b.v)}; }
+__device__ __forceinline__ Ex<float> operator*(Ex<float> a, Ex<float> b) { return {__fmul_rn(a.v, b.v)}; }
+__device__ __forceinline__ Ex<float> operator/(Ex<float> a, Ex<float> b) { return {__fdiv_rn(a.v, b.v)}; }
+template <class T> __device__ __forceinline__ Ex<T> operator-(Ex<T> a) { return {-a.v}; }
+
+template <class V> struct Num;  // constants and conversions for V
+template <> struct Num<double> {
+  using R = double;
+  __device__ static __forceinline__ double c(double x) { return x; }
+  __device__ static __forceinline__ double raw(double x) { return x; }
+  __device__ static __forceinline__ double wrap(double x) { return x; }
+};
+template <> struct Num<float> {
+  using R = float;
+  __device__ static __forceinline__ float c(double x) { return (float)x; }
+  __device__ static __forceinline__ float raw(float x) { return x; }
+  __device__ static __forceinline__ float wrap(float x) { return x; }
+};
+template <class T> struct Num<Ex<T>> {
+  using R = T;
+  __device__ static __forceinline__ Ex<T> c(double x) { return {(T)x}; }
+  __device__ static __forceinline__ T raw(Ex<T> x) { return x.v; }
+  __device__ static __forceinline__ Ex<T> wrap(T x) { return {x}; }
+};
+
+// ------------------------------------------------------------ storage forms
+// F64: double storage / double arithmetic (reference DOUBLE_P build).
+// F32: float storage of f - w / float arithmetic (reference default build).
+// F16: binary16 storage of scale*(f - w) / float arithmetic.
+struct F64 {
+  using S = double; using R = double; using V = Ex<double>;
+  static constexpr int id = 0;
+  __device__ static __forceinline__ R dec(S s, R) { return s; }
+  __device__ static __forceinline__ S enc(R r, R) { return r; }
+};
+struct F32 {
+  using S = float; using R = float; using V = Ex<float>;
+  static constexpr int id = 1;
+  __device__ static __forceinline__ R dec(S s, R) { return s; }
+  __device__ static __forceinline__ S enc(R r, R) { return r; }
+};
+struct F16 {
+  using S = __half; using R = float; using V = Ex<float>;
+  static constexpr int id = 2;
+  // inv and scale are exact powers of two: the multiply only moves the exponent
+  __device__ static __forceinline__ R dec(S s, R inv) { return __fmul_rn(__half2float(s), inv); }
+  __device__ static __forceinline__ S enc(R r, R scale) { return __float2half_rn(__fmul_rn(r, scale)); }
+};
+
+// ----------------------------------------------------------------- geometry
+// Population q of a lattice is a dense nx*ny*nz block (rows padded to sx
+// elements) starting at base + q*qs. Cell (i,j,k) is at i + sx*(j + ny*k).
+struct Geo {
+  int nx, ny, nz;
+  int sx;          // row pitch, elements (multiple of 32)
+  long long qs;    // population stride, elements
+};
+
+template <class S> struct Pops { S* p[Q]; };
+
+// --------------------------------------------------------- per-cell physics
+// Moments and equilibrium deviation in the reference's evaluation order
+// (SRC/col_MC.F90:133-219). x: pulled deviations; e: equilibrium deviations.
+template <class V>
+__device__ __forceinline__ V equilibrium(const V (&x)[Q], V (&e)[Q], V& vxo, V& vyo, V& vzo) {
+  using N = Num<V>;
+  const V uno = N::c(1.0), cte1 = N::c(1.0), cte0 = uno - cte1;
+  const V rf = N::c(3.0), qf = N::c(1.5), tre = N::c(3.0);
+  const V p0 = N::c(1.0 / 3.0), p1 = N::c(1.0 / 18.0), p2 = N::c(1.0 / (3.0 * 3.0 * (1.0 + 3.0)));
+  V rho = x[0] + x[1] + x[2] + x[3] + x[4] + x[5] + x[6] + x[7]
+        + x[8] + x[9] + x[10] + x[11] + x[12] + x[13] + x[14] + x[15]
+        + x[16] + x[17] + x[18] + cte1;
+  V rhoinv = uno / rho;
+  V vx = (x[0] + x[1] + x[2] + x[3] + x[4] - x[9] - x[10] - x[11] - x[12] - x[13]) * rhoinv;
+  V vy = (x[2] + x[6] + x[7] + x[8] + x[11] - x[0] - x[9] - x[15] - x[16] - x[17]) * rhoinv;
+  V vz = (x[3] + x[5] + x[6] + x[12] + x[17] - x[1] - x[8] - x[10] - x[14] - x[15]) * rhoinv;
+  vxo = vx; vyo = vy; vzo = vz;
+  V vx2 = vx * vx, vy2 = vy * vy, vz2 = vz * vz;
+  V vsq = vx2 + vy2 + vz2;
+  V vxpy = vx + vy; V qxpy = cte0 + qf * (tre * vxpy * vxpy - vsq);
+  V vxmy = vx - vy; V qxmy = cte0 + qf * (tre * vxmy * vxmy - vsq);
+  V vxpz = vx + vz; V qxpz = cte0 + qf * (tre * vxpz * vxpz - vsq);
+  V vxmz = vx - vz; V qxmz = cte0 + qf * (tre * vxmz * vxmz - vsq);
+  V vypz = vy + vz; V qypz = cte0 + qf * (tre * vypz * vypz - vsq);
+  V vymz = vy - vz; V qymz = cte0 + qf * (tre * vymz * vymz - vsq);
+  V qx = cte0 + qf * (tre * vx2 - vsq);
+  V qy = cte0 + qf * (tre * vy2 - vsq);
+  V qz = cte0 + qf * (tre * vz2 - vsq);
+  V q0 = cte0 + qf * (-vsq);
+  vx = rf * vx; vy = rf * vy; vz = rf * vz;
+  vxpy = rf * vxpy; vxmy = rf * vxmy; vxpz = rf * vxpz;
+  vxmz = rf * vxmz; vypz = rf * vypz; vymz = rf * vymz;
+  V rp0 = rho * p0, rp1 = rho * p1, rp2 = rho * p2;
+  V s2 = cte1 * (rp2 - p2), s1 = cte1 * (rp1 - p1), s0 = cte1 * (rp0 - p0);
+  e[0]  = rp2 * (vxmy + qxmy) + s2;
+  e[1]  = rp2 * (vxmz + qxmz) + s2;
+  e[2]  = rp2 * (vxpy + qxpy) + s2;
+  e[3]  = rp2 * (vxpz + qxpz) + s2;
+  e[4]  = rp1 * (vx + qx) + s1;
+  e[5]  = rp1 * (vz + qz) + s1;
+  e[6]  = rp2 * (vypz + qypz) + s2;
+  e[7]  = rp1 * (vy + qy) + s1;
+  e[8]  = rp2 * (vymz + qymz) + s2;
+  e[9]  = rp2 * (-vxpy + qxpy) + s2;
+  e[10] = rp2 * (-vxpz + qxpz) + s2;
+  e[11] = rp2 * (-vxmy + qxmy) + s2;
+  e[12] = rp2 * (-vxmz + qxmz) + s2;
+  e[13] = rp1 * (-vx + qx) + s1;
+  e[14] = rp1 * (-vz + qz) + s1;
+  e[15] = rp2 * (-vypz + qypz) + s2;
+  e[16] = rp1 * (-vy + qy) + s1;
+  e[17] = rp2 * (-vymz + qymz) + s2;
+  e[18] = rp0 * q0 + s0;
+  return rho;
+}
+
+// BGK relaxation x <- x - omega*(x - e) (SRC/col_MC.F90:333-351), in place.
+template <class V>
+__device__ __forceinline__ void collide(V (&x)[Q], V omega) {
+  V e[Q], vx, vy, vz;
+  (void)equilibrium<V>(x, e, vx, vy, vz);
+#pragma unroll
+  for (int q = 0; q < Q; ++q) x[q] = x[q] - omega * (x[q] - e[q]);
+}
+
+// Ptotal = Pi_neq : Pi_neq with doubled off-diagonals (SRC/dissipation.F90:171-247).
+template <class V>
+__device__ __forceinline__ V ptotal(const V (&x)[Q], const V (&e)[Q]) {
+  using N = Num<V>;
+  V n[18];
+#pragma unroll
+  for (int q = 0; q < 18; ++q) n[q] = x[q] - e[q];
+  V Pxx = n[0] + n[1] + n[2] + n[3] + n[4] + n[9] + n[10] + n[11] + n[12] + n[13];
+  V Pyy = n[0] + n[2] + n[6] + n[7] + n[8] + n[9] + n[11] + n[15] + n[16] + n[17];
+  V Pzz = n[1] + n[3] + n[5] + n[6] + n[8] + n[10] + n[12] + n[14] + n[15] + n[17];
+  V Pxz = -n[1] + n[3] + n[10] - n[12];
+  V Pxy = -n[0] + n[2] + n[9] - n[11];
+  V Pyz = n[6] - n[8] + n[15] - n[17];
+  const V two = N::c(2.0);
+  return (Pxx * Pxx) + (Pyy * Pyy) + (Pzz * Pzz) + (two * Pxy * Pxy) + (two * Pxz * Pxz) + (two * Pyz * Pyz);
+}
+
+}  // namespace bgk

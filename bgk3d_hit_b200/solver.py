@@ -1,0 +1,239 @@
+"""Host-side mirror of the reference's subroutine interface.
+
+``BGK3D`` exposes the reference's per-rank call sequence
+(SRC/bgk3d_HIT.F90:74-146) as methods with the same names:
+
+    input / hencol / alloca  -> BGK3D(...) or BGK3D.from_input("bgk.input")
+    init                     -> init()                 (Taylor-Green, SRC/init.F90)
+    boundaries(itime)        -> boundaries(itime)      (no-op: wrap in kernel)
+    col_MC(itime)            -> col_MC(itime)
+    diagnostic(itime, ...)   -> diagnostic(itime)      (gated by icheck)
+    diagno(itime)            -> diagno(itime)
+    dissipation(itime)       -> dissipation(itime)
+
+``run_loop`` replays the program's time loop and writes ``diagno.dat``
+(fort.70, SRC/diagno.F90:137) and ``dissipation.dat`` (fort.71,
+SRC/dissipation.F90:261-269) with the reference's columns and formats.
+
+Every call goes through the C-ABI of ``libbgk3d.so``; nothing is computed on
+the host.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+
+import numpy as np
+
+from . import _abi
+from ._abi import BgkDiag, BgkParams, check
+
+_STORE_DTYPES = {_abi.BGK_FP64: np.float64, _abi.BGK_FP32DEV: np.float32, _abi.BGK_FP16DEV: np.float16}
+
+
+def read_namelist(path: str) -> dict:
+    """Reads the reference's ``&parameters`` namelist (SRC/input.F90:41-47)."""
+    text = open(path).read()
+    m = re.search(r"&parameters(.*?)/", text, re.S | re.I)
+    if not m:
+        raise ValueError(f"no &parameters group in {path}")
+    out = {}
+    for key, val in re.findall(r"(\w+)\s*=\s*([^,\s/]+)", m.group(1)):
+        v = val.strip().rstrip(",").replace("d", "e").replace("D", "e")
+        try:
+            out[key.lower()] = int(v)
+        except ValueError:
+            out[key.lower()] = float(v)
+    return out
+
+
+class BGK3D:
+    """One periodic D3Q19 box on one GPU, driven like the reference program."""
+
+    def __init__(self, lx: int = 64, ly: int | None = None, lz: int | None = None, *, svisc: float = 0.01,
+                 u0: float = 0.05, precision: str = "fp64", scheme: str = "two_lattice", icheck: int = 10,
+                 mode: str = "corrected", fp16_scale: float = 0.0, device: int = 0, omega: float | None = None,
+                 extras: bool = True):
+        self._lib = _abi.load()
+        p = BgkParams()
+        check(self._lib.bgk_params_default(C.byref(p)), "bgk_params_default")
+        p.lx, p.ly, p.lz = lx, ly or lx, lz or lx
+        p.svisc, p.u0 = svisc, u0
+        p.precision = _abi.PRECISIONS[precision] if isinstance(precision, str) else int(precision)
+        p.scheme = _abi.SCHEMES[scheme] if isinstance(scheme, str) else int(scheme)
+        p.mode = _abi.MODES[mode] if isinstance(mode, str) else int(mode)
+        p.icheck, p.fp16_scale, p.device, p.extras = icheck, fp16_scale, device, int(extras)
+        if omega is not None:
+            p.use_omega, p.omega = 1, omega
+        self.params = p
+        self._h = C.c_void_p()
+        check(self._lib.bgk_create(C.byref(p), C.byref(self._h)), "bgk_create")
+        self.shape = (p.lx, p.ly, p.lz)
+        self.dtype = _STORE_DTYPES[p.precision]
+
+    # ----------------------------------------------------------- set-up
+    @classmethod
+    def from_input(cls, path: str, **kw) -> "BGK3D":
+        """input + hencol + alloca from a bgk.input namelist (one rank)."""
+        nl = read_namelist(path)
+        for ax in ("x", "y", "z"):
+            if nl.get("proc_" + ax, 1) != 1:
+                raise ValueError("one box per GPU: proc_x = proc_y = proc_z = 1")
+        return cls(nl["lx"], nl["ly"], nl["lz"], svisc=nl["svisc"], u0=nl["u0"], icheck=nl.get("icheck", 100), **kw)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.bgk_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def ncell(self) -> int:
+        lx, ly, lz = self.shape
+        return lx * ly * lz
+
+    def init(self):
+        """Taylor-Green vortex (SRC/init.F90:23-163)."""
+        check(self._lib.bgk_init_tgv(self._h), "bgk_init_tgv")
+
+    def init_velocity(self, u, v, w, rho: float = 1.0):
+        lx, ly, lz = self.shape
+        a = [np.ascontiguousarray(np.asarray(x, dtype=np.float64).reshape(lz, ly, lx)) for x in (u, v, w)]
+        dp = C.POINTER(C.c_double)
+        check(self._lib.bgk_init_velocity(self._h, a[0].ctypes.data_as(dp), a[1].ctypes.data_as(dp),
+                                          a[2].ctypes.data_as(dp), rho), "bgk_init_velocity")
+
+    # -------------------------------------------------------- time loop
+    def boundaries(self, itime: int):
+        check(self._lib.bgk_boundaries(self._h, itime), "bgk_boundaries")
+
+    def col_MC(self, itime: int):
+        check(self._lib.bgk_col_mc(self._h, itime), "bgk_col_mc")
+
+    def run(self, nsteps: int):
+        check(self._lib.bgk_run(self._h, nsteps), "bgk_run")
+
+    def diagnostic(self, itime: int) -> dict | None:
+        """Gated like SRC/diagnostic.F90:37: None when mod(itime, icheck) != 0."""
+        d = BgkDiag()
+        rc = check(self._lib.bgk_diagnostic(self._h, itime, C.byref(d)), "bgk_diagnostic",
+                   ok=(_abi.BGK_OK, _abi.BGK_SKIPPED))
+        return None if rc == _abi.BGK_SKIPPED else d.as_dict()
+
+    def diagno(self, itime: int) -> np.ndarray:
+        out = np.zeros(5)
+        check(self._lib.bgk_diagno(self._h, itime, out.ctypes.data_as(C.POINTER(C.c_double))), "bgk_diagno")
+        return out
+
+    def dissipation(self, itime: int) -> np.ndarray:
+        out = np.zeros(4)
+        check(self._lib.bgk_dissipation(self._h, itime, out.ctypes.data_as(C.POINTER(C.c_double))),
+              "bgk_dissipation")
+        return out
+
+    # ------------------------------------------------------------ data
+    def populations(self) -> np.ndarray:
+        lx, ly, lz = self.shape
+        out = np.empty((19, lz, ly, lx), dtype=self.dtype)
+        check(self._lib.bgk_get_populations(self._h, out.ctypes.data), "bgk_get_populations")
+        return out
+
+    def set_populations(self, pops: np.ndarray):
+        lx, ly, lz = self.shape
+        a = np.ascontiguousarray(np.asarray(pops, dtype=self.dtype).reshape(19, lz, ly, lx))
+        check(self._lib.bgk_put_populations(self._h, a.ctypes.data), "bgk_put_populations")
+
+    def deviations(self) -> np.ndarray:
+        lx, ly, lz = self.shape
+        out = np.empty((19, lz, ly, lx), dtype=np.float64)
+        check(self._lib.bgk_get_deviations(self._h, out.ctypes.data_as(C.POINTER(C.c_double))),
+              "bgk_get_deviations")
+        return out
+
+    def velocity(self):
+        lx, ly, lz = self.shape
+        u, v, w = (np.empty((lz, ly, lx)) for _ in range(3))
+        dp = C.POINTER(C.c_double)
+        check(self._lib.bgk_get_velocity(self._h, u.ctypes.data_as(dp), v.ctypes.data_as(dp),
+                                         w.ctypes.data_as(dp)), "bgk_get_velocity")
+        return u, v, w
+
+    def spectrum(self, nbins: int | None = None) -> np.ndarray:
+        nb = nbins or (max(self.shape) // 2 + 1)
+        out = np.zeros(nb)
+        check(self._lib.bgk_spectrum(self._h, nb, out.ctypes.data_as(C.POINTER(C.c_double))), "bgk_spectrum")
+        return out
+
+    # ------------------------------------------------------- properties
+    def _getd(self, fn):
+        v = C.c_double()
+        check(getattr(self._lib, fn)(self._h, C.byref(v)), fn)
+        return v.value
+
+    def _getll(self, fn):
+        v = C.c_longlong()
+        check(getattr(self._lib, fn)(self._h, C.byref(v)), fn)
+        return v.value
+
+    @property
+    def omega(self) -> float:
+        return self._getd("bgk_get_omega")
+
+    @property
+    def scale(self) -> float:
+        return self._getd("bgk_get_scale")
+
+    @property
+    def step(self) -> int:
+        return self._getll("bgk_get_step")
+
+    @property
+    def device_bytes(self) -> int:
+        return self._getll("bgk_get_device_bytes")
+
+    @property
+    def launch_count(self) -> int:
+        return self._getll("bgk_get_launch_count")
+
+    @property
+    def stream(self) -> int:
+        return self._lib.bgk_get_stream(self._h) or 0
+
+    def synchronize(self):
+        check(self._lib.bgk_synchronize(self._h), "bgk_synchronize")
+
+
+def run_loop(box: BGK3D, itfin: int, out_dir: str | None = None, itstart: int = 1):
+    """Replays the time loop of SRC/bgk3d_HIT.F90:127-146 (boundaries, col_MC,
+    diagnostic) and returns the diagnostic records; with out_dir, writes
+    diagno.dat and dissipation.dat in the reference's formats (i8, e14.6)."""
+    recs = []
+    for itime in range(itstart, itfin + 1):
+        box.boundaries(itime)
+        box.col_MC(itime)
+        d = box.diagnostic(itime)
+        if d is not None:
+            recs.append(d)
+    if out_dir:
+        os.makedirs(out_dir, exist_ok=True)
+        with open(os.path.join(out_dir, "diagno.dat"), "w") as f70, \
+                open(os.path.join(out_dir, "dissipation.dat"), "w") as f71:
+            for d in recs:
+                # format 1004: i8, 5(e14.6,1x) -- itime, xtot, ytot, ztot, rtot, stot
+                f70.write("%8d" % d["itime"] + "".join(" %14.6E" % x for x in (
+                    d["ux_mean"], d["uy_mean"], d["uz_mean"], d["rho_mean"], d["ke_mean"])) + "\n")
+                f71.write("%8d" % d["itime"] + "".join(" %14.6E" % x for x in (
+                    d["t"], d["tke_norm"], d["diss"])) + "\n")
+    return recs

@@ -1,0 +1,196 @@
+/*
+ * bgk3d.h - C-ABI of the B200 implementation of the BGK3D_HIT time-step hot
+ * path (D3Q19 BGK, triply periodic box, one GPU).
+ *
+ * The entry points mirror the reference's Fortran call sequence
+ * (SRC/bgk3d_HIT.F90:74-92 set-up, :127-146 time loop):
+ *
+ *     input + setup_MPI + hencol + alloca  ->  bgk_create
+ *     init                                 ->  bgk_init_tgv / bgk_init_velocity
+ *     do itime = 1, itfin
+ *        boundaries(itime)                 ->  bgk_boundaries   (no-op: the
+ *                                              periodic wrap is inside the kernel)
+ *        col_MC(itime)                     ->  bgk_col_mc
+ *        diagnostic(itime, icheck, ...)    ->  bgk_diagnostic
+ *     end do
+ *     finalize                             ->  bgk_destroy
+ *
+ * Conventions
+ *  - Every function returns BGK_OK (0) on success, a negative BGK_ERR_* code
+ *    on error, and never exits the process (the reference stops instead,
+ *    e.g. SRC/input.F90:66-82). bgk_last_error() gives a message.
+ *  - Host arrays are Fortran order (i fastest) without ghost layers; a
+ *    population array is q-major: element (q, i, j, k), q = 0..18 for the
+ *    reference's a01..a19, sits at q*lx*ly*lz + i + lx*(j + ly*k).
+ *  - Populations are deviations f_q - w_q (the reference's default storage,
+ *    cte1 = 1 in SRC/col_MC.F90:86-90), in the stored precision; the FP16
+ *    form stores scale*(f_q - w_q).
+ *  - A context is not thread-safe. Its work runs in order on one CUDA stream
+ *    owned by the context; calls that return host data synchronise it.
+ *  - The library allocates all device memory it uses in bgk_create and on
+ *    first use of a diagnostic, and frees it in bgk_destroy.
+ */
+#ifndef BGK3D_H
+#define BGK3D_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BGK_OK 0
+#define BGK_SKIPPED 1          /* bgk_diagnostic: not a diagnostic step */
+#define BGK_ERR_INVALID (-1)   /* bad argument or parameter */
+#define BGK_ERR_CUDA (-2)      /* CUDA runtime error */
+#define BGK_ERR_NOMEM (-3)     /* device allocation failed */
+#define BGK_ERR_STATE (-4)     /* call out of order (e.g. step before init) */
+#define BGK_ERR_NONFINITE (-5) /* diagnostics found non-finite moments */
+
+/* Storage / arithmetic forms (SRC/precision.F90:19-38 has DOUBLE_P and the
+   single-precision default; the FP16 form has no working reference
+   counterpart, SRC/precision.F90:40-43). */
+#define BGK_FP64 0    /* double storage, double arithmetic */
+#define BGK_FP32DEV 1 /* float storage of f - w, float arithmetic */
+#define BGK_FP16DEV 2 /* binary16 storage of scale*(f - w), float arithmetic */
+
+/* Update schemes. */
+#define BGK_TWO_LATTICE 0 /* pull stream-collide a -> b and swap, SRC/col_MC.F90:98-421 */
+#define BGK_AA 1          /* in-place AA pattern, one lattice (no reference counterpart) */
+
+/* Modes. */
+#define BGK_CORRECTED 0 /* TGV init in double with rho = 1; diagno sums ztot */
+#define BGK_FAITHFUL 1  /* TGV init with single-precision coordinates, pi and the
+                           pressure-consistent crho (SRC/init.F90:42,84-95);
+                           diagno keeps ztot = ytot + zj (SRC/diagno.F90:110) */
+
+typedef struct bgk_ctx bgk_ctx;
+
+/* Run parameters: the reference's namelist &parameters (SRC/input.F90:41-47)
+   restricted to one box, plus the build-time choices of the reference
+   (precision, scheme) as run-time values. */
+typedef struct {
+  int lx, ly, lz;      /* box size (SRC/input.F90:61-63; one rank: l = lx ...) */
+  double svisc;        /* kinematic viscosity nu; omega = 2/(6 nu + 1), SRC/hencol.F90:31 */
+  double u0;           /* reference velocity (TGV amplitude, dissipation.dat normalisation) */
+  int precision;       /* BGK_FP64 / BGK_FP32DEV / BGK_FP16DEV */
+  int scheme;          /* BGK_TWO_LATTICE / BGK_AA */
+  int icheck;          /* diagnostic interval (SRC/diagnostic.F90:37) */
+  int mode;            /* BGK_CORRECTED / BGK_FAITHFUL */
+  double fp16_scale;   /* FP16 form: scale (power of two); 0 = chosen at init */
+  int device;          /* CUDA device ordinal */
+  int use_omega;       /* 1: use `omega` below instead of the svisc formula */
+  double omega;        /* collision frequency override (e.g. 0 = pure streaming) */
+  int extras;          /* 1: bgk_diagnostic also computes enstrophy */
+} bgk_params;
+
+/* Diagnostics of one step, in FP64. */
+typedef struct {
+  int itime;
+  /* diagno.dat columns, SRC/diagno.F90:117-137 (means over the box of the
+     local, un-pulled populations) */
+  double rho_mean, ux_mean, uy_mean, uz_mean, ke_mean;
+  /* dissipation.dat columns, SRC/dissipation.F90:261-269 (pulled populations):
+     t = itime*dt, tke_norm = sum(0.5|u|^2)/(l m n u0^2), diss = sum(2 svisc Ptotal) */
+  double t, tke_norm, diss;
+  double tke;          /* sum(0.5|u|^2) over the pulled populations, unnormalised */
+  double enstrophy;    /* mean 0.5|curl u|^2 (central differences), no reference counterpart */
+  double eps_strain;   /* mean 2 nu S:S, S = -3 omega Pi_neq/(2 rho), no reference counterpart */
+  long long nonfinite; /* cells with non-finite local rho or u */
+} bgk_diag;
+
+/* Fills defaults: 64^3, svisc 0.01, u0 0.05, FP64, two-lattice, icheck 10,
+   corrected mode, device 0, extras on. */
+int bgk_params_default(bgk_params* p);
+
+/* = input + setup_MPI + hencol + alloca (SRC/bgk3d_HIT.F90:74-89). Validates
+   the parameters, selects the device, allocates the lattice(s). */
+int bgk_create(const bgk_params* p, bgk_ctx** out);
+
+/* = finalize's teardown (SRC/finalize.F90): frees everything. NULL is ok. */
+int bgk_destroy(bgk_ctx* ctx);
+
+/* = init (SRC/init.F90:23-163): Taylor-Green vortex with amplitude u0. */
+int bgk_init_tgv(bgk_ctx* ctx);
+
+/* Equilibrium initial condition from a host velocity field (three arrays of
+   lx*ly*lz doubles, Fortran order) at uniform density rho; the per-cell
+   arithmetic of SRC/init.F90:97-137 with crho = rho. Used for decaying HIT. */
+int bgk_init_velocity(bgk_ctx* ctx, const double* u, const double* v, const double* w, double rho);
+
+/* = boundaries(itime) (SRC/boundaries.F90:23-107, default STEP3 variant
+   SRC/bcond.comm.step3.F90:29-316). The single periodic box needs no halo
+   exchange: every kernel wraps its indices. Kept so that the call sequence is
+   unchanged; validates the context and returns BGK_OK. */
+int bgk_boundaries(bgk_ctx* ctx, int itime);
+
+/* = col_MC(itime) (SRC/col_MC.F90:34-444): one fused pull-stream + BGK
+   collide step over the box, including the a <-> b swap (two-lattice) or the
+   layout flip (AA). Asynchronous. */
+int bgk_col_mc(bgk_ctx* ctx, int itime);
+
+/* Runs nsteps consecutive bgk_boundaries + bgk_col_mc steps. Asynchronous. */
+int bgk_run(bgk_ctx* ctx, int nsteps);
+
+/* = diagnostic(itime, icheck, ...) (SRC/diagnostic.F90:25-75): when
+   mod(itime, icheck) == 0 computes diagno + dissipation (+ enstrophy when
+   params.extras) into *out and returns BGK_OK (or BGK_ERR_NONFINITE when
+   out->nonfinite > 0); otherwise returns BGK_SKIPPED and leaves *out alone.
+   Synchronous. */
+int bgk_diagnostic(bgk_ctx* ctx, int itime, bgk_diag* out);
+
+/* = diagno(itime) (SRC/diagno.F90:28-154): out[5] = {mean rho, mean ux,
+   mean uy, mean uz, mean 0.5|u|^2}. Ungated. */
+int bgk_diagno(bgk_ctx* ctx, int itime, double* out5);
+
+/* = dissipation(itime) (SRC/dissipation.F90:176-280): out[4] = {itime*dt,
+   tke_norm, diss, tke}. Ungated. */
+int bgk_dissipation(bgk_ctx* ctx, int itime, double* out4);
+
+/* Current populations in the reference's meaning (post-collision a_q of
+   SRC/col_MC.F90 after the swap), stored type (double / float / binary16
+   bits), q-major Fortran order. */
+int bgk_get_populations(bgk_ctx* ctx, void* host19);
+int bgk_put_populations(bgk_ctx* ctx, const void* host19);
+/* Same as bgk_get_populations, decoded to double deviations f_q - w_q. */
+int bgk_get_deviations(bgk_ctx* ctx, double* host19);
+/* Local velocity u = j/rho of every cell (as in SRC/diagno.F90:100-104). */
+int bgk_get_velocity(bgk_ctx* ctx, double* u, double* v, double* w);
+
+/* Shell-averaged kinetic-energy spectrum of the local velocity field:
+   E[k] = sum over wavevectors with round(|k|) == k of 0.5|u_hat|^2 / N^2,
+   k = 0..nbins-1 (cuFFT). No reference counterpart. */
+int bgk_spectrum(bgk_ctx* ctx, int nbins, double* ek);
+
+/* Scale of the FP16 form (1.0 for the other forms). */
+int bgk_get_scale(const bgk_ctx* ctx, double* scale);
+/* omega in use (SRC/hencol.F90:31 in the form's arithmetic, or the override). */
+int bgk_get_omega(const bgk_ctx* ctx, double* omega);
+/* Number of steps taken since the last init. */
+int bgk_get_step(const bgk_ctx* ctx, long long* step);
+/* Device bytes allocated by the context. */
+int bgk_get_device_bytes(const bgk_ctx* ctx, long long* bytes);
+/* Number of kernel launches issued by the context so far. */
+int bgk_get_launch_count(const bgk_ctx* ctx, long long* count);
+/* The context's CUDA stream (a cudaStream_t), for event timing by callers. */
+void* bgk_get_stream(const bgk_ctx* ctx);
+/* Waits for all work of the context. */
+int bgk_synchronize(bgk_ctx* ctx);
+
+/* Streaming-only calibrator, the single-box equivalent of do_somethingGPU
+   (SRC/do_somethingGPU.F90:37-100) without the MPI barrier: out1(i,j,k) =
+   in1(i-1,j,k), out2 = in2(i,j-1,k), out3 = in3(i,j,k-1) with periodic wrap
+   (reverse = 1: +1 shifts, the REVERSE validation mode). Device pointers of
+   dense Fortran-order nx*ny*nz arrays of elem_bytes = 2, 4 or 8; stream may
+   be NULL (default stream). Asynchronous. */
+int bgk_shift3(const void* in1, const void* in2, const void* in3, void* out1, void* out2, void* out3, int nx, int ny,
+               int nz, int elem_bytes, int reverse, void* stream);
+
+const char* bgk_strerror(int code);
+/* Message of the last error on this thread. */
+const char* bgk_last_error(void);
+/* Library version string. */
+const char* bgk_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BGK3D_H */

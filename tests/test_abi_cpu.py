@@ -1,0 +1,128 @@
+"""CPU tests of the C-ABI library (no GPU needed): it loads, exports every
+entry point of include/bgk3d.h with the declared struct layouts, validates
+parameters before touching a device, and the host helpers behave."""
+import ctypes as C
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "bgk3d.h")
+
+
+def header_functions():
+    txt = open(HEADER).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(bgk_\w+)\s*\(", txt)))
+
+
+def test_library_exports_every_declared_symbol(bgk):
+    lib = bgk.load()
+    names = header_functions()
+    assert len(names) >= 25
+    for n in names:
+        assert hasattr(lib, n), n
+    out = subprocess.run(["nm", "-D", "--defined-only", bgk._abi.LIB_PATH], capture_output=True, text=True).stdout
+    exported = set(re.findall(r" T (bgk_\w+)", out))
+    assert set(names) <= exported
+    # the ctypes prototypes cover exactly the header
+    assert sorted(n for n, _, _ in bgk._abi.PROTOTYPES) == names
+
+
+def test_struct_layout_matches_header(bgk, tmp_path):
+    src = tmp_path / "layout.c"
+    src.write_text(
+        '#include <stddef.h>\n#include <stdio.h>\n#include "bgk3d.h"\n'
+        "#define P(T, f) printf(\"%s.%s %zu\\n\", #T, #f, offsetof(T, f));\n"
+        "int main(void) {\n"
+        'printf("bgk_params %zu\\nbgk_diag %zu\\n", sizeof(bgk_params), sizeof(bgk_diag));\n'
+        + "".join(f"P(bgk_params, {f})\n" for f, _ in bgk._abi.BgkParams._fields_)
+        + "".join(f"P(bgk_diag, {f})\n" for f, _ in bgk._abi.BgkDiag._fields_)
+        + "return 0; }\n")
+    exe = tmp_path / "layout"
+    cc = "/usr/bin/gcc" if os.path.exists("/usr/bin/gcc") else "gcc"
+    subprocess.run([cc, "-I", os.path.dirname(HEADER), str(src), "-o", str(exe)], check=True)
+    lines = dict(l.split() for l in subprocess.run([str(exe)], capture_output=True, text=True).stdout.splitlines())
+    assert int(lines["bgk_params"]) == C.sizeof(bgk._abi.BgkParams)
+    assert int(lines["bgk_diag"]) == C.sizeof(bgk._abi.BgkDiag)
+    for T, S in (("bgk_params", bgk._abi.BgkParams), ("bgk_diag", bgk._abi.BgkDiag)):
+        for f, _ in S._fields_:
+            assert int(lines[f"{T}.{f}"]) == getattr(S, f).offset, (T, f)
+
+
+def _params(bgk, **kw):
+    p = bgk._abi.BgkParams()
+    assert bgk.load().bgk_params_default(C.byref(p)) == 0
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+def test_defaults(bgk):
+    p = _params(bgk)
+    assert (p.lx, p.ly, p.lz, p.precision, p.scheme, p.icheck, p.mode) == (64, 64, 64, 0, 0, 10, 0)
+    assert p.svisc == 0.01 and p.u0 == 0.05 and p.extras == 1
+
+
+@pytest.mark.parametrize("bad", [
+    dict(lx=0), dict(lz=-3), dict(precision=7), dict(scheme=2), dict(mode=5), dict(icheck=0),
+    dict(svisc=0.0), dict(svisc=-1.0), dict(svisc=float("nan")), dict(use_omega=1, omega=2.5),
+    dict(fp16_scale=3.0), dict(fp16_scale=-2.0), dict(u0=float("inf")), dict(lx=4096, ly=4096, lz=4096),
+])
+def test_create_rejects_bad_parameters_before_touching_a_device(bgk, bad):
+    lib = bgk.load()
+    h = C.c_void_p()
+    rc = lib.bgk_create(C.byref(_params(bgk, **bad)), C.byref(h))
+    assert rc == bgk._abi.BGK_ERR_INVALID
+    assert not h.value
+    assert lib.bgk_last_error()
+
+
+def test_null_arguments(bgk):
+    lib = bgk.load()
+    assert lib.bgk_create(None, None) == bgk._abi.BGK_ERR_INVALID
+    assert lib.bgk_col_mc(None, 1) == bgk._abi.BGK_ERR_INVALID
+    assert lib.bgk_boundaries(None, 1) == bgk._abi.BGK_ERR_INVALID
+    assert lib.bgk_diagnostic(None, 1, None) == bgk._abi.BGK_ERR_INVALID
+    assert lib.bgk_destroy(None) == 0
+    assert lib.bgk_get_stream(None) is None
+    assert lib.bgk_shift3(None, None, None, None, None, None, 1, 1, 1, 8, 0, None) == bgk._abi.BGK_ERR_INVALID
+
+
+def test_strerror_and_version(bgk):
+    lib = bgk.load()
+    assert b"sm_100a" in lib.bgk_version()
+    for code in (0, 1, -1, -2, -3, -4, -5):
+        assert lib.bgk_strerror(code) != b"unknown error"
+
+
+def test_namelist_reader(tmp_path):
+    from bgk3d_hit_b200 import read_namelist
+
+    f = tmp_path / "bgk.input"
+    f.write_text("&parameters\nlx = 48\nly = 40\nlz = 32\nproc_x = 1\nproc_y = 1\nproc_z = 1\n"
+                 "u0 = 0.05\nsvisc = 1.0d-2\nitfin = 500\nicheck = 10 /\n")
+    nl = read_namelist(str(f))
+    assert (nl["lx"], nl["ly"], nl["lz"], nl["itfin"], nl["icheck"]) == (48, 40, 32, 500, 10)
+    assert nl["svisc"] == 0.01 and nl["u0"] == 0.05
+
+
+def test_hit_generator_properties():
+    from bgk3d_hit_b200.hit import divergence_spectral, hit_velocity
+
+    u, v, w = hit_velocity(32, k0=4, u_rms=0.03, seed=1234)
+    assert u.shape == (32, 32, 32)
+    assert np.sqrt((u * u + v * v + w * w).mean() / 3) == pytest.approx(0.03, rel=1e-12)
+    assert divergence_spectral(u, v, w) < 1e-14
+    u2, _, _ = hit_velocity(32, k0=4, u_rms=0.03, seed=1234)
+    assert np.array_equal(u, u2)
+    u3, _, _ = hit_velocity(32, k0=4, u_rms=0.03, seed=1235)
+    assert not np.array_equal(u, u3)
+    # shell spectrum peaks near k0 (E ~ k^4 exp(-2 (k/k0)^2) peaks at k0)
+    k = np.sqrt(sum(g ** 2 for g in np.meshgrid(*[np.fft.fftfreq(32, 1 / 32)] * 3, indexing="ij")))
+    e = sum(np.abs(np.fft.fftn(a)) ** 2 for a in (u, v, w))
+    shells = np.bincount(np.rint(k).astype(int).ravel(), e.ravel())
+    assert abs(int(np.argmax(shells)) - 4) <= 1

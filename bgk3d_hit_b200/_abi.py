@@ -80,6 +80,8 @@ PROTOTYPES = [
     ("bgk_get_stream", _vp, [_vp]),
     ("bgk_synchronize", _i, [_vp]),
     ("bgk_shift3", _i, [_vp, _vp, _vp, _vp, _vp, _vp, _i, _i, _i, _i, _i, _vp]),
+    ("bgk_diagnostics_noalloc", _i, [C.POINTER(_vp), _i, _i, _i, _i, _i, _d, _d, _d, _d, _i, _i,
+                                     C.POINTER(BgkDiag), _vp]),
     ("bgk_strerror", C.c_char_p, [_i]),
     ("bgk_last_error", C.c_char_p, []),
     ("bgk_version", C.c_char_p, []),

@@ -227,6 +227,8 @@ int compute_diag(bgk_ctx* c, int itime, bgk_diag* out, int want_extras) {
 
 }  // namespace
 
+void bgk::set_last_error(const char* msg) { set_err("%s", msg); }
+
 extern "C" {
 
 int bgk_params_default(bgk_params* p) {

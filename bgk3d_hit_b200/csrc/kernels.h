@@ -63,4 +63,7 @@ cudaError_t launch_spectrum_bins(const void* fft_out, int form, int nx, int ny, 
 cudaError_t launch_shift3(const void* const in[3], void* const out[3], int nx, int ny, int nz, int elem_bytes,
                           int reverse, cudaStream_t st);
 
+// Sets the message returned by bgk_last_error() on this thread.
+void set_last_error(const char* msg);
+
 }  // namespace bgk

@@ -184,6 +184,30 @@ int bgk_synchronize(bgk_ctx* ctx);
 int bgk_shift3(const void* in1, const void* in2, const void* in3, void* out1, void* out2, void* out3, int nx, int ny,
                int nz, int elem_bytes, int reverse, void* stream);
 
+/* Diagnostics without any allocation, for callers that cannot allocate device
+   memory once their time loop runs (a driver whose device arrays all belong
+   to another runtime, such as an OpenACC data region, or an application that
+   gives all device memory to its own pool; cudaMalloc can fail on a full
+   device and synchronises it). No counterpart in the reference.
+   Computes the bgk_diagnostic fields except enstrophy (left 0) over caller-
+   owned device populations in the reference's meaning: pops19[q] is the
+   device base of population q, cell (i,j,k) at i + pitch_x*(j + ly*k), stored
+   as `precision` (FP16: scale fp16_scale). svisc and omega enter the
+   dissipation and strain sums, u0 and itime the dissipation.dat columns, mode
+   the diagno ztot convention. Runs on the calling thread's current device and
+   on `stream` (NULL: default stream), then synchronises that stream.
+   Scratch: one file-scope device array of 94,808 bytes per GPU (held until the
+   process exits), whatever the box size; boxes are limited to
+   pitch_x*ly*lz < 2^31 cells per population and larger ones are rejected with
+   BGK_ERR_INVALID. The array keeps the last call's contents; every slot is
+   rewritten before it is read, but calls that overlap on the GPU (concurrent
+   streams, threads) race on it. The first call on a device looks up the
+   array's device address (cudaGetSymbolAddress): make that first call before
+   any stream capture. Calls no cudaMalloc or cudaFree. */
+int bgk_diagnostics_noalloc(const void* const* pops19, int lx, int ly, int lz, int pitch_x, int precision,
+                            double svisc, double omega, double u0, double fp16_scale, int mode, int itime,
+                            bgk_diag* out, void* stream);
+
 const char* bgk_strerror(int code);
 /* Message of the last error on this thread. */
 const char* bgk_last_error(void);

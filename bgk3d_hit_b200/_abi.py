@@ -35,7 +35,7 @@ class BgkParams(C.Structure):
         ("svisc", C.c_double), ("u0", C.c_double),
         ("precision", C.c_int), ("scheme", C.c_int), ("icheck", C.c_int), ("mode", C.c_int),
         ("fp16_scale", C.c_double), ("device", C.c_int),
-        ("use_omega", C.c_int), ("omega", C.c_double), ("extras", C.c_int),
+        ("use_omega", C.c_int), ("omega", C.c_double), ("extras", C.c_int), ("kernel", C.c_int),
     ]
 
 
@@ -82,6 +82,7 @@ PROTOTYPES = [
     ("bgk_shift3", _i, [_vp, _vp, _vp, _vp, _vp, _vp, _i, _i, _i, _i, _i, _vp]),
     ("bgk_diagnostics_noalloc", _i, [C.POINTER(_vp), _i, _i, _i, _i, _i, _d, _d, _d, _d, _i, _i,
                                      C.POINTER(BgkDiag), _vp]),
+    ("bgk_debug_stall_next_step", _i, [_vp]),
     ("bgk_strerror", C.c_char_p, [_i]),
     ("bgk_last_error", C.c_char_p, []),
     ("bgk_version", C.c_char_p, []),

@@ -19,7 +19,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 OUT = os.path.join(HERE, "libbgk3d.so")
-SOURCES = ["kernels.cu", "bgk_abi.cu", "noalloc.cu"]
+SOURCES = ["kernels.cu", "rows.cu", "bgk_abi.cu", "noalloc.cu"]
 HEADERS = ["lattice.cuh", "kernels.h"]
 ARCH = "-gencode=arch=compute_100a,code=sm_100a"
 

@@ -62,6 +62,8 @@ struct bgk_ctx {
   double* totals = nullptr;
   double* h_tot = nullptr;  // pinned
   unsigned int* d_max = nullptr;
+  int* d_err = nullptr;     // set on the device when a pipelined kernel's wait ran out
+  int* h_err = nullptr;     // pinned copy
   void* vel = nullptr;
   void* stage = nullptr;
   size_t stage_bytes = 0;
@@ -167,6 +169,18 @@ int set_scale_from_max(bgk_ctx* c) {
 
 int init_layout(const bgk_ctx* c) { return c->scheme == BGK_AA ? LAY_AAE : LAY_TWO; }
 
+// Synchronises the stream and reports a bounded wait of a pipelined kernel
+// that ran out (the step it belonged to did not complete).
+int sync_and_check(bgk_ctx* c) {
+  CK(cudaMemcpyAsync(c->h_err, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  if (*c->h_err) {
+    set_err("a stream-collide step gave up waiting for its row copies; populations are invalid");
+    return BGK_ERR_CUDA;
+  }
+  return BGK_OK;
+}
+
 int compute_diag(bgk_ctx* c, int itime, bgk_diag* out, int want_extras) {
   const bool extras = want_extras && c->p.extras;
   if (extras) {
@@ -187,7 +201,8 @@ int compute_diag(bgk_ctx* c, int itime, bgk_diag* out, int want_extras) {
     c->launches++;
   }
   CK(cudaMemcpyAsync(c->h_tot, c->totals, (ND + 1) * sizeof(double), cudaMemcpyDeviceToHost, c->st));
-  CK(cudaStreamSynchronize(c->st));
+  int rc = sync_and_check(c);
+  if (rc) return rc;
   const double* t = c->h_tot;
   const double N = (double)ncell(c);
   out->itime = itime;
@@ -246,6 +261,7 @@ int bgk_params_default(bgk_params* p) {
   p->use_omega = 0;
   p->omega = 0.0;
   p->extras = 1;
+  p->kernel = 0;
   return BGK_OK;
 }
 
@@ -271,6 +287,10 @@ int bgk_create(const bgk_params* p, bgk_ctx** out) {
   }
   if (p->mode != BGK_CORRECTED && p->mode != BGK_FAITHFUL) {
     set_err("invalid mode %d", p->mode);
+    return BGK_ERR_INVALID;
+  }
+  if (p->kernel != 0 && p->kernel != 1 && p->kernel != 2 && p->kernel != 4 && p->kernel != 8) {
+    set_err("kernel must be 0, 1, 2, 4 or 8 (got %d)", p->kernel);
     return BGK_ERR_INVALID;
   }
   if (p->icheck < 1) {
@@ -355,6 +375,13 @@ int bgk_create(const bgk_params* p, bgk_ctx** out) {
   if (rc) return fail(rc);
   rc = dev_alloc(c, (void**)&c->d_max, sizeof(unsigned int), "scale probe");
   if (rc) return fail(rc);
+  rc = dev_alloc(c, (void**)&c->d_err, sizeof(int), "error flag");
+  if (rc) return fail(rc);
+  e = cudaMemsetAsync(c->d_err, 0, sizeof(int), c->st);
+  if (e != cudaSuccess) return fail(cuda_fail(e, "cudaMemset"));
+  e = cudaMallocHost((void**)&c->h_err, sizeof(int));
+  if (e != cudaSuccess) return fail(cuda_fail(e, "cudaMallocHost"));
+  c->A.err = c->B.err = c->d_err;
   e = cudaMallocHost((void**)&c->h_tot, (ND + 1) * sizeof(double));
   if (e != cudaSuccess) return fail(cuda_fail(e, "cudaMallocHost"));
   c->lay = init_layout(c);
@@ -372,6 +399,8 @@ int bgk_destroy(bgk_ctx* c) {
   cudaFree(c->partials);
   cudaFree(c->totals);
   cudaFree(c->d_max);
+  cudaFree(c->d_err);
+  if (c->h_err) cudaFreeHost(c->h_err);
   cudaFree(c->vel);
   cudaFree(c->stage);
   cudaFree(c->fft_buf);
@@ -397,6 +426,7 @@ int bgk_init_tgv(bgk_ctx* c) {
   }
   CK(launch_init_tgv(c->A, lay, c->p.u0, faithful, c->scale, nullptr, c->st));
   c->launches++;
+  CK(cudaMemsetAsync(c->d_err, 0, sizeof(int), c->st));
   c->lay = lay;
   c->step = 0;
   c->initialized = 1;
@@ -444,6 +474,7 @@ int bgk_init_velocity(bgk_ctx* c, const double* u, const double* v, const double
       c->launches++;
     }
   }
+  CK(cudaMemsetAsync(c->d_err, 0, sizeof(int), c->st));
   CK(cudaStreamSynchronize(c->st));
   c->lay = lay;
   c->step = 0;
@@ -462,7 +493,7 @@ int bgk_col_mc(bgk_ctx* c, int itime) {
   if (rc) return rc;
   CK(cudaSetDevice(c->p.device));
   if (c->scheme == BGK_TWO_LATTICE) {
-    CK(launch_two_lattice(c->A, c->B, c->omega, c->scale, 0, c->st));
+    CK(launch_two_lattice(c->A, c->B, c->omega, c->scale, c->p.kernel, c->st));
     // pointer swap of pops 01..18, SRC/col_MC.F90:364-421
     for (int q = 0; q < Q - 1; ++q) {
       void* t = c->A.p[q];
@@ -471,11 +502,23 @@ int bgk_col_mc(bgk_ctx* c, int itime) {
     }
   } else {
     const int odd = c->lay == LAY_AAE;
-    CK(launch_aa(c->A, odd, c->omega, c->scale, c->st));
+    CK(launch_aa(c->A, odd, c->omega, c->scale, c->p.kernel, c->st));
     c->lay = odd ? LAY_AAN : LAY_AAE;
   }
   c->launches++;
   c->step++;
+  c->A.stall = c->B.stall = 0;
+  return BGK_OK;
+}
+
+int bgk_debug_stall_next_step(bgk_ctx* c) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (c->p.kernel != 8) {
+    set_err("bgk_debug_stall_next_step needs the row-pipelined kernel (params.kernel = 8)");
+    return BGK_ERR_INVALID;
+  }
+  c->A.stall = c->B.stall = 1;
   return BGK_OK;
 }
 
@@ -542,8 +585,7 @@ int bgk_get_populations(bgk_ctx* c, void* host) {
     c->launches++;
     CK(cudaMemcpyAsync((char*)host + q * n * c->es, c->stage, n * c->es, cudaMemcpyDeviceToHost, c->st));
   }
-  CK(cudaStreamSynchronize(c->st));
-  return BGK_OK;
+  return sync_and_check(c);
 }
 
 int bgk_get_deviations(bgk_ctx* c, double* host) {
@@ -559,8 +601,7 @@ int bgk_get_deviations(bgk_ctx* c, double* host) {
     c->launches++;
     CK(cudaMemcpyAsync(host + q * n, c->stage, n * 8, cudaMemcpyDeviceToHost, c->st));
   }
-  CK(cudaStreamSynchronize(c->st));
-  return BGK_OK;
+  return sync_and_check(c);
 }
 
 int bgk_put_populations(bgk_ctx* c, const void* host) {
@@ -577,6 +618,7 @@ int bgk_put_populations(bgk_ctx* c, const void* host) {
     CK(launch_import(c->A, lay, q, c->stage, c->st));
     c->launches++;
   }
+  CK(cudaMemsetAsync(c->d_err, 0, sizeof(int), c->st));
   CK(cudaStreamSynchronize(c->st));
   c->lay = lay;
   if (!c->initialized) c->step = 0;
@@ -703,8 +745,7 @@ int bgk_synchronize(bgk_ctx* c) {
   int rc = check_ctx(c);
   if (rc) return rc;
   CK(cudaSetDevice(c->p.device));
-  CK(cudaStreamSynchronize(c->st));
-  return BGK_OK;
+  return sync_and_check(c);
 }
 
 int bgk_shift3(const void* in1, const void* in2, const void* in3, void* out1, void* out2, void* out3, int nx, int ny,

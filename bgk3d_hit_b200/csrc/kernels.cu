@@ -55,9 +55,8 @@ static int grid_1d(long long n, int threads, int cap) {
 
 // ------------------------------------------------------------- two lattice
 template <class F>
-__global__ void __launch_bounds__(256) k_two(Pops<const typename F::S> src, Pops<typename F::S> dst, Geo g,
-                                             typename F::R omega, typename F::R scale, typename F::R inv) {
-  using S = typename F::S; using V = typename F::V; using N = Num<V>;
+__global__ void __launch_bounds__(256) k_two(Pops<const typename F::S> src, Pops<typename F::S> dst, Geo g, StepK K) {
+  using S = typename F::S;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int k = blockIdx.z;
@@ -65,7 +64,7 @@ __global__ void __launch_bounds__(256) k_two(Pops<const typename F::S> src, Pops
   const int im = i == 0 ? g.nx - 1 : i - 1, ip = i == g.nx - 1 ? 0 : i + 1;
   const int jm = j == 0 ? g.ny - 1 : j - 1, jp = j == g.ny - 1 ? 0 : j + 1;
   const int km = k == 0 ? g.nz - 1 : k - 1, kp = k == g.nz - 1 ? 0 : k + 1;
-  V x[Q];
+  S v[Q];
 #pragma unroll
   for (int q = 0; q < Q; ++q) {
     // pull from (i - cx, j - cy, k - cz), SRC/col_MC.F90:113-131
@@ -73,13 +72,176 @@ __global__ void __launch_bounds__(256) k_two(Pops<const typename F::S> src, Pops
     const int jj = cyq(q) > 0 ? jm : (cyq(q) < 0 ? jp : j);
     const int kk = czq(q) > 0 ? km : (czq(q) < 0 ? kp : k);
     const int off = ii + g.sx * (jj + g.ny * kk);
-    const S s = (q == Q - 1) ? dst.p[Q - 1][off] : ldg(src.p[q] + off);
-    x[q] = N::wrap(F::dec(s, inv));
+    v[q] = (q == Q - 1) ? dst.p[Q - 1][off] : ldg(src.p[q] + off);
   }
-  collide<V>(x, N::wrap(omega));
+  F::cell(v, K);
   const int o = i + g.sx * (j + g.ny * k);
 #pragma unroll
-  for (int q = 0; q < Q; ++q) dst.p[q][o] = F::enc(N::raw(x[q]), scale);
+  for (int q = 0; q < Q; ++q) dst.p[q][o] = v[q];
+}
+
+// FP16 two-lattice step with 4 cells per thread and 8-byte accesses. A row of
+// nx cells is handled by tpr = nx/4 consecutive threads (tpr a power of two).
+// x-shifted pulls take the element that crosses a thread boundary from the
+// neighbouring lane (warp shuffle); across warp boundaries (tpr > 32) lanes 0
+// and 31 load it. Each cell's arithmetic is F16::cell's (moments16, pair16, rest16).
+__device__ __forceinline__ unsigned short ldg_u16(const __half* p) {
+  return __ldg(reinterpret_cast<const unsigned short*>(p));
+}
+__device__ __forceinline__ unsigned h2u(__half2 h) { return *reinterpret_cast<unsigned*>(&h); }
+__device__ __forceinline__ float2 u2f2(unsigned u) { return __half22float2(*reinterpret_cast<__half2*>(&u)); }
+
+__global__ void __launch_bounds__(256, 2) k_two_f16v(Pops<const __half> src, Pops<__half> dst, Geo g, StepK K,
+                                                  int log_tpr) {
+  const int tpr = 1 << log_tpr;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = t >> log_tpr, pos = t & (tpr - 1);
+  const int k = blockIdx.y;
+  if (j >= g.ny) return;  // whole warps: ny*tpr is a multiple of 32
+  const int lane = threadIdx.x & 31;
+  const int i0 = pos * 4;
+  const int jm = j == 0 ? g.ny - 1 : j - 1, jp = j == g.ny - 1 ? 0 : j + 1;
+  const int km = k == 0 ? g.nz - 1 : k - 1, kp = k == g.nz - 1 ? 0 : k + 1;
+  int src_prev, src_next;
+  bool load_prev = false, load_next = false;
+  if (tpr >= 32) {
+    src_prev = (lane + 31) & 31;
+    src_next = (lane + 1) & 31;
+    load_prev = lane == 0;
+    load_next = lane == 31;
+  } else {
+    src_prev = pos == 0 ? lane + tpr - 1 : lane - 1;
+    src_next = pos == tpr - 1 ? lane - tpr + 1 : lane + 1;
+  }
+  const int i_prev = pos == 0 ? g.nx - 1 : i0 - 1;
+  const int i_next = pos == tpr - 1 ? 0 : i0 + 4;
+  uint2 Y[Q];  // four cells' stored values per population, cell m in half m
+#pragma unroll
+  for (int q = 0; q < Q; ++q) {
+    const int jj = cyq(q) > 0 ? jm : (cyq(q) < 0 ? jp : j);
+    const int kk = czq(q) > 0 ? km : (czq(q) < 0 ? kp : k);
+    const __half* p = (q == Q - 1 ? (const __half*)dst.p[Q - 1] : src.p[q]) + g.sx * (jj + g.ny * kk);
+    const uint2 A = (q == Q - 1) ? *reinterpret_cast<const uint2*>(p + i0) : __ldg(reinterpret_cast<const uint2*>(p + i0));
+    if (cxq(q) == 0) {
+      Y[q] = A;
+    } else if (cxq(q) > 0) {  // cells need elements i0-1 .. i0+2
+      unsigned prev = __shfl_sync(0xffffffffu, A.y >> 16, src_prev);
+      if (load_prev) prev = ldg_u16(p + i_prev);
+      Y[q].x = __byte_perm(A.x, prev, 0x1054);
+      Y[q].y = __byte_perm(A.x, A.y, 0x5432);
+    } else {  // cells need elements i0+1 .. i0+4
+      unsigned next = __shfl_sync(0xffffffffu, A.x & 0xffffu, src_next);
+      if (load_next) next = ldg_u16(p + i_next);
+      Y[q].x = __byte_perm(A.x, A.y, 0x5432);
+      Y[q].y = __byte_perm(A.y, next, 0x5432);
+    }
+  }
+  Mom16 M[4];
+#pragma unroll
+  for (int m = 0; m < 4; ++m) {
+    float y[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      const float2 f = u2f2(m < 2 ? Y[q].x : Y[q].y);
+      y[q] = (m & 1) ? f.y : f.x;
+    }
+    M[m] = moments16(y, K);
+  }
+  const int o = i0 + g.sx * (j + g.ny * k);
+#pragma unroll
+  for (int q = 0; q < 9; ++q) {
+    const int r = oppq(q);
+    const float2 a = u2f2(Y[q].x), b = u2f2(Y[q].y), c = u2f2(Y[r].x), d = u2f2(Y[r].y);
+    float p0, p1, p2, p3, o0, o1, o2, o3;
+    pair16(q, a.x, c.x, M[0], K.om1, p0, o0);
+    pair16(q, a.y, c.y, M[1], K.om1, p1, o1);
+    pair16(q, b.x, d.x, M[2], K.om1, p2, o2);
+    pair16(q, b.y, d.y, M[3], K.om1, p3, o3);
+    *reinterpret_cast<uint2*>(dst.p[q] + o) =
+        make_uint2(h2u(__floats2half2_rn(p0, p1)), h2u(__floats2half2_rn(p2, p3)));
+    *reinterpret_cast<uint2*>(dst.p[r] + o) =
+        make_uint2(h2u(__floats2half2_rn(o0, o1)), h2u(__floats2half2_rn(o2, o3)));
+  }
+  {
+    const float2 a = u2f2(Y[Q - 1].x), b = u2f2(Y[Q - 1].y);
+    *reinterpret_cast<uint2*>(dst.p[Q - 1] + o) =
+        make_uint2(h2u(__floats2half2_rn(rest16(a.x, M[0], K.om1), rest16(a.y, M[1], K.om1))),
+                   h2u(__floats2half2_rn(rest16(b.x, M[2], K.om1), rest16(b.y, M[3], K.om1))));
+  }
+}
+
+// Same with 2 cells per thread and 4-byte accesses (tpr = nx/2 threads per row).
+__global__ void __launch_bounds__(256, 4) k_two_f16v2(Pops<const __half> src, Pops<__half> dst, Geo g, StepK K,
+                                                   int log_tpr) {
+  const int tpr = 1 << log_tpr;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = t >> log_tpr, pos = t & (tpr - 1);
+  const int k = blockIdx.y;
+  if (j >= g.ny) return;  // whole warps: ny*tpr is a multiple of 32
+  const int lane = threadIdx.x & 31;
+  const int i0 = pos * 2;
+  const int jm = j == 0 ? g.ny - 1 : j - 1, jp = j == g.ny - 1 ? 0 : j + 1;
+  const int km = k == 0 ? g.nz - 1 : k - 1, kp = k == g.nz - 1 ? 0 : k + 1;
+  int src_prev, src_next;
+  bool load_prev = false, load_next = false;
+  if (tpr >= 32) {
+    src_prev = (lane + 31) & 31;
+    src_next = (lane + 1) & 31;
+    load_prev = lane == 0;
+    load_next = lane == 31;
+  } else {
+    src_prev = pos == 0 ? lane + tpr - 1 : lane - 1;
+    src_next = pos == tpr - 1 ? lane - tpr + 1 : lane + 1;
+  }
+  const int i_prev = pos == 0 ? g.nx - 1 : i0 - 1;
+  const int i_next = pos == tpr - 1 ? 0 : i0 + 2;
+  unsigned Y[Q];  // two cells' stored values per population, cell m in half m
+#pragma unroll
+  for (int q = 0; q < Q; ++q) {
+    const int jj = cyq(q) > 0 ? jm : (cyq(q) < 0 ? jp : j);
+    const int kk = czq(q) > 0 ? km : (czq(q) < 0 ? kp : k);
+    const __half* p = (q == Q - 1 ? (const __half*)dst.p[Q - 1] : src.p[q]) + g.sx * (jj + g.ny * kk);
+    const unsigned A = (q == Q - 1) ? *reinterpret_cast<const unsigned*>(p + i0)
+                                    : __ldg(reinterpret_cast<const unsigned*>(p + i0));
+    if (cxq(q) == 0) {
+      Y[q] = A;
+    } else if (cxq(q) > 0) {  // cells need elements i0-1, i0
+      unsigned prev = __shfl_sync(0xffffffffu, A >> 16, src_prev);
+      if (load_prev) prev = ldg_u16(p + i_prev);
+      Y[q] = __byte_perm(A, prev, 0x1054);
+    } else {  // cells need elements i0+1, i0+2
+      unsigned next = __shfl_sync(0xffffffffu, A & 0xffffu, src_next);
+      if (load_next) next = ldg_u16(p + i_next);
+      Y[q] = __byte_perm(A, next, 0x5432);
+    }
+  }
+  Mom16 M[2];
+#pragma unroll
+  for (int m = 0; m < 2; ++m) {
+    float y[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      const float2 f = u2f2(Y[q]);
+      y[q] = m ? f.y : f.x;
+    }
+    M[m] = moments16(y, K);
+  }
+  const int o = i0 + g.sx * (j + g.ny * k);
+#pragma unroll
+  for (int q = 0; q < 9; ++q) {
+    const int r = oppq(q);
+    const float2 a = u2f2(Y[q]), c = u2f2(Y[r]);
+    float p0, p1, o0, o1;
+    pair16(q, a.x, c.x, M[0], K.om1, p0, o0);
+    pair16(q, a.y, c.y, M[1], K.om1, p1, o1);
+    *reinterpret_cast<unsigned*>(dst.p[q] + o) = h2u(__floats2half2_rn(p0, p1));
+    *reinterpret_cast<unsigned*>(dst.p[r] + o) = h2u(__floats2half2_rn(o0, o1));
+  }
+  {
+    const float2 a = u2f2(Y[Q - 1]);
+    *reinterpret_cast<unsigned*>(dst.p[Q - 1] + o) =
+        h2u(__floats2half2_rn(rest16(a.x, M[0], K.om1), rest16(a.y, M[1], K.om1)));
+  }
 }
 
 // --------------------------------------------------------------- AA pattern
@@ -88,15 +250,14 @@ __global__ void __launch_bounds__(256) k_two(Pops<const typename F::S> src, Pops
 // Each thread reads exactly the locations it writes, so the update is
 // race-free in place.
 template <class F, bool ODD>
-__global__ void __launch_bounds__(256) k_aa(Pops<typename F::S> a, Geo g, typename F::R omega,
-                                            typename F::R scale, typename F::R inv) {
-  using V = typename F::V; using N = Num<V>;
+__global__ void __launch_bounds__(256) k_aa(Pops<typename F::S> a, Geo g, StepK K) {
+  using S = typename F::S;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int k = blockIdx.z;
   if (i >= g.nx || j >= g.ny) return;
   const int o = i + g.sx * (j + g.ny * k);
-  V x[Q];
+  S v[Q];
   int off[Q];
   if (ODD) {
     const int im = i == 0 ? g.nx - 1 : i - 1, ip = i == g.nx - 1 ? 0 : i + 1;
@@ -111,18 +272,18 @@ __global__ void __launch_bounds__(256) k_aa(Pops<typename F::S> a, Geo g, typena
       off[q] = ii + g.sx * (jj + g.ny * kk);
     }
 #pragma unroll
-    for (int q = 0; q < Q; ++q) x[q] = N::wrap(F::dec(a.p[oppq(q)][off[q]], inv));
+    for (int q = 0; q < Q; ++q) v[q] = a.p[oppq(q)][off[q]];
   } else {
 #pragma unroll
-    for (int q = 0; q < Q; ++q) x[q] = N::wrap(F::dec(a.p[q][o], inv));
+    for (int q = 0; q < Q; ++q) v[q] = a.p[q][o];
   }
-  collide<V>(x, N::wrap(omega));
+  F::cell(v, K);
   if (ODD) {
 #pragma unroll
-    for (int q = 0; q < Q; ++q) a.p[q][off[oppq(q)]] = F::enc(N::raw(x[q]), scale);
+    for (int q = 0; q < Q; ++q) a.p[q][off[oppq(q)]] = v[q];
   } else {
 #pragma unroll
-    for (int q = 0; q < Q; ++q) a.p[oppq(q)][o] = F::enc(N::raw(x[q]), scale);
+    for (int q = 0; q < Q; ++q) a.p[oppq(q)][o] = v[q];
   }
 }
 
@@ -473,42 +634,92 @@ template <class S> static Pops<S> pops_of(const Lattice& L) {
   return p;
 }
 
+StepK make_stepk(int form, double omega, double scale) {
+  StepK k{};
+  k.omega = omega;
+  k.omega_f = (float)omega;
+  k.inv = (float)(1.0 / scale);
+  k.om1 = 1.0f - (float)omega;
+  const double w[3] = {1.0 / 3.0, 1.0 / 18.0, 1.0 / 36.0};
+  for (int c = 0; c < 3; ++c) k.kw[c] = (float)((double)(float)omega * scale * w[c]);
+  (void)form;
+  return k;
+}
+
+// log2(nx/V) when the V-cells-per-thread FP16 kernel applies, else -1.
+static int f16v_log_tpr(const Geo& g, int V) {
+  if (g.nx % V) return -1;
+  const int tpr = g.nx / V;
+  if (tpr & (tpr - 1)) return -1;
+  if (((long long)g.ny * tpr) % 32) return -1;
+  int l = 0;
+  while ((1 << l) < tpr) ++l;
+  return l;
+}
+
 template <class F>
-static cudaError_t two_impl(const Lattice& s, const Lattice& d, double omega, double scale, cudaStream_t st) {
-  using S = typename F::S; using R = typename F::R;
+static cudaError_t two_impl(const Lattice& s, const Lattice& d, const StepK& K, int variant, cudaStream_t st) {
+  using S = typename F::S;
   Pops<const S> ps = pops_of<const S>(s);
   Pops<S> pd = pops_of<S>(d);
   pd.p[Q - 1] = (S*)s.p[Q - 1];  // pop 19 in place (SRC/col_MC.F90:351)
+  if (variant == 8) {
+    bool launched = false;
+    cudaError_t e = launch_rows(s, d, ROW_TWO, K, st, &launched);
+    if (e != cudaSuccess || launched) return e;
+  }
+  // automatic choice (variant 0): one cell per thread, the fastest measured
+  // on B200 for every form at 256^3 (FP16: 62.0 GLUPS vs 61.2 / 62.3 for two /
+  // four cells per thread and 44.6 for the row pipeline)
+  if (F::id == FORM_F16 && (variant == 2 || variant == 4)) {
+    const int V = variant;
+    const int lt = f16v_log_tpr(s.g, V);
+    if (lt >= 0) {
+      const long long threads = (long long)s.g.ny << lt;
+      dim3 grid((unsigned)((threads + 255) / 256), s.g.nz);
+      Pops<__half> ph = pops_of<__half>(d);
+      ph.p[Q - 1] = (__half*)s.p[Q - 1];
+      if (V == 4) k_two_f16v<<<grid, 256, 0, st>>>(pops_of<const __half>(s), ph, s.g, K, lt);
+      else k_two_f16v2<<<grid, 256, 0, st>>>(pops_of<const __half>(s), ph, s.g, K, lt);
+      return cudaGetLastError();
+    }
+  }
   Shape sh = cell_shape(s.g);
-  k_two<F><<<sh.grid, sh.block, 0, st>>>(ps, pd, s.g, (R)omega, (R)scale, (R)(1.0 / scale));
+  k_two<F><<<sh.grid, sh.block, 0, st>>>(ps, pd, s.g, K);
   return cudaGetLastError();
 }
 
 cudaError_t launch_two_lattice(const Lattice& src, const Lattice& dst, double omega, double scale, int variant,
                                cudaStream_t st) {
-  (void)variant;
+  const StepK K = make_stepk(src.form, omega, scale);
   switch (src.form) {
-    case FORM_F64: return two_impl<F64>(src, dst, omega, scale, st);
-    case FORM_F32: return two_impl<F32>(src, dst, omega, scale, st);
-    case FORM_F16: return two_impl<F16>(src, dst, omega, scale, st);
+    case FORM_F64: return two_impl<F64>(src, dst, K, variant, st);
+    case FORM_F32: return two_impl<F32>(src, dst, K, variant, st);
+    case FORM_F16: return two_impl<F16>(src, dst, K, variant, st);
   }
   return cudaErrorInvalidValue;
 }
 
 template <class F>
-static cudaError_t aa_impl(const Lattice& a, int odd, double omega, double scale, cudaStream_t st) {
-  using S = typename F::S; using R = typename F::R;
+static cudaError_t aa_impl(const Lattice& a, int odd, const StepK& K, int variant, cudaStream_t st) {
+  using S = typename F::S;
+  if (variant == 8) {
+    bool launched = false;
+    cudaError_t e = launch_rows(a, a, odd ? ROW_AA_ODD : ROW_AA_EVEN, K, st, &launched);
+    if (e != cudaSuccess || launched) return e;
+  }
   Shape sh = cell_shape(a.g);
-  if (odd) k_aa<F, true><<<sh.grid, sh.block, 0, st>>>(pops_of<S>(a), a.g, (R)omega, (R)scale, (R)(1.0 / scale));
-  else k_aa<F, false><<<sh.grid, sh.block, 0, st>>>(pops_of<S>(a), a.g, (R)omega, (R)scale, (R)(1.0 / scale));
+  if (odd) k_aa<F, true><<<sh.grid, sh.block, 0, st>>>(pops_of<S>(a), a.g, K);
+  else k_aa<F, false><<<sh.grid, sh.block, 0, st>>>(pops_of<S>(a), a.g, K);
   return cudaGetLastError();
 }
 
-cudaError_t launch_aa(const Lattice& a, int odd, double omega, double scale, cudaStream_t st) {
+cudaError_t launch_aa(const Lattice& a, int odd, double omega, double scale, int variant, cudaStream_t st) {
+  const StepK K = make_stepk(a.form, omega, scale);
   switch (a.form) {
-    case FORM_F64: return aa_impl<F64>(a, odd, omega, scale, st);
-    case FORM_F32: return aa_impl<F32>(a, odd, omega, scale, st);
-    case FORM_F16: return aa_impl<F16>(a, odd, omega, scale, st);
+    case FORM_F64: return aa_impl<F64>(a, odd, K, variant, st);
+    case FORM_F32: return aa_impl<F32>(a, odd, K, variant, st);
+    case FORM_F16: return aa_impl<F16>(a, odd, K, variant, st);
   }
   return cudaErrorInvalidValue;
 }

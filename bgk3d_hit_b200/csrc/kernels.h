@@ -16,21 +16,34 @@ enum Layout { LAY_TWO = 0, LAY_AAE = 1, LAY_AAN = 2 };
 struct Lattice {
   int form;
   Geo g;
-  void* p[Q];  // population base pointers
+  void* p[Q];          // population base pointers
+  int* err = nullptr;  // device flag set by a pipelined kernel whose wait ran out
+  int stall = 0;       // test hook: the next pipelined launch waits on a barrier nothing arms
 };
+
+// Modes of the row-pipelined kernel (rows.cu).
+enum RowMode { ROW_TWO = 0, ROW_AA_EVEN = 1, ROW_AA_ODD = 2 };
 
 // Number of accumulated diagnostic quantities (see kernels.cu).
 constexpr int ND = 10;
 constexpr int DIAG_BLOCKS = 148 * 4;
 constexpr int DIAG_THREADS = 256;
 
+// Collision constants of one launch for a form.
+StepK make_stepk(int form, double omega, double scale);
+
 // Two-lattice fused pull-stream + collide: src -> dst (pops 1..18), pop 19 in
-// place in src.
+// place in src. variant: 0 automatic, 1 one cell per thread, 2 / 4 cells per
+// thread for the FP16 form, 8 row pipeline with TMA bulk copies (each falls
+// back to 1 where the box does not fit it).
 cudaError_t launch_two_lattice(const Lattice& src, const Lattice& dst, double omega, double scale, int variant,
                                cudaStream_t st);
 // AA pattern: even (local read, reversed local write) or odd (pull from
-// neighbours' opposite slots, push to neighbours).
-cudaError_t launch_aa(const Lattice& a, int odd, double omega, double scale, cudaStream_t st);
+// neighbours' opposite slots, push to neighbours). variant as above (1 or 8).
+cudaError_t launch_aa(const Lattice& a, int odd, double omega, double scale, int variant, cudaStream_t st);
+// Row-pipelined kernel; *launched = false when the box does not fit it.
+cudaError_t launch_rows(const Lattice& src, const Lattice& dst, int mode, const StepK& K, cudaStream_t st,
+                        bool* launched);
 
 // Initial conditions (write layout `lay`, which must be LAY_TWO or LAY_AAE).
 // mx != nullptr: only measure max |f - w| into *mx (bits of a float), no store.

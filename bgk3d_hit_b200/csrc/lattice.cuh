@@ -69,27 +69,142 @@ template <class T> struct Num<Ex<T>> {
 };
 
 // ------------------------------------------------------------ storage forms
+// Per-launch constants of the collision, for every form.
+struct StepK {
+  double omega;   // F64
+  float omega_f;  // F32
+  float inv;      // F16: 1/scale
+  float om1;      // F16: 1 - omega
+  float kw[3];    // F16: omega*scale*w for w = 1/3, 1/18, 1/36
+};
+
+// Weight class of population q: 0 -> 1/3 (rest), 1 -> 1/18, 2 -> 1/36.
+__host__ __device__ constexpr int wclass(int q) {
+  return q == 18 ? 0 : ((q == 4 || q == 5 || q == 7 || q == 13 || q == 14 || q == 16) ? 1 : 2);
+}
+
+template <class V>
+__device__ __forceinline__ void collide(V (&x)[Q], V omega);
+
 // F64: double storage / double arithmetic (reference DOUBLE_P build).
 // F32: float storage of f - w / float arithmetic (reference default build).
-// F16: binary16 storage of scale*(f - w) / float arithmetic.
+// Both use the reference's evaluation order with every operation rounded.
 struct F64 {
   using S = double; using R = double; using V = Ex<double>;
   static constexpr int id = 0;
   __device__ static __forceinline__ R dec(S s, R) { return s; }
   __device__ static __forceinline__ S enc(R r, R) { return r; }
+  __device__ static __forceinline__ void cell(S (&s)[Q], const StepK& k) {
+    V x[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) x[q] = V{s[q]};
+    collide<V>(x, V{k.omega});
+#pragma unroll
+    for (int q = 0; q < Q; ++q) s[q] = x[q].v;
+  }
 };
 struct F32 {
   using S = float; using R = float; using V = Ex<float>;
   static constexpr int id = 1;
   __device__ static __forceinline__ R dec(S s, R) { return s; }
   __device__ static __forceinline__ S enc(R r, R) { return r; }
+  __device__ static __forceinline__ void cell(S (&s)[Q], const StepK& k) {
+    V x[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) x[q] = V{s[q]};
+    collide<V>(x, V{k.omega_f});
+#pragma unroll
+    for (int q = 0; q < Q; ++q) s[q] = x[q].v;
+  }
 };
+
+// F16: binary16 storage of y = scale*(f - w), float arithmetic. The FP16 form
+// has no reference counterpart (SRC/precision.F90:40-43 stops on HALF_P), so
+// its collision is written for this storage: it works on the scaled values y
+// directly, keeps the density deviation dr = sum(f - w) apart from 1, treats
+// each pair of opposite directions together and uses fused multiply-adds:
+//   dr = sum(y)/scale, u = j(y)/(scale*(1 + dr)), a = -1.5|u|^2,
+//   for the pair (q, opp q) with cu = c_q.u:
+//     Q2 = (4.5 cu) cu + a,  P(+-) = +-3 cu + Q2   (f_eq/w - 1 = dr + (1+dr) P)
+//   y' = (1 - omega) y + kd + kr P, kd = K dr, kr = K + kd, K = omega*scale*w.
+// Sums and roundings are fixed (moments16, pair16) and restated by the oracle.
+struct Mom16 { float ux, uy, uz, a, kd[3], kr[3]; };
+
+__device__ __forceinline__ Mom16 moments16(const float (&y)[Q], const StepK& k) {
+  const float sp = __fadd_rn(__fadd_rn(__fadd_rn(y[0], y[1]), __fadd_rn(y[2], y[3])), y[4]);
+  const float sm = __fadd_rn(__fadd_rn(__fadd_rn(y[9], y[10]), __fadd_rn(y[11], y[12])), y[13]);
+  const float s0 = __fadd_rn(__fadd_rn(__fadd_rn(__fadd_rn(y[5], y[6]), __fadd_rn(y[7], y[8])),
+                                       __fadd_rn(__fadd_rn(y[14], y[15]), __fadd_rn(y[16], y[17]))),
+                             y[18]);
+  const float sum = __fadd_rn(__fadd_rn(sp, sm), s0);
+  const float jx = __fsub_rn(sp, sm);
+  const float jyp = __fadd_rn(__fadd_rn(__fadd_rn(y[2], y[6]), __fadd_rn(y[7], y[8])), y[11]);
+  const float jym = __fadd_rn(__fadd_rn(__fadd_rn(y[0], y[9]), __fadd_rn(y[15], y[16])), y[17]);
+  const float jzp = __fadd_rn(__fadd_rn(__fadd_rn(y[3], y[5]), __fadd_rn(y[6], y[12])), y[17]);
+  const float jzm = __fadd_rn(__fadd_rn(__fadd_rn(y[1], y[8]), __fadd_rn(y[10], y[14])), y[15]);
+  Mom16 m;
+  const float dr = __fmul_rn(sum, k.inv);
+  const float r = __fdiv_rn(k.inv, __fadd_rn(1.0f, dr));
+  m.ux = __fmul_rn(jx, r);
+  m.uy = __fmul_rn(__fsub_rn(jyp, jym), r);
+  m.uz = __fmul_rn(__fsub_rn(jzp, jzm), r);
+  const float usq = __fmaf_rn(m.uz, m.uz, __fmaf_rn(m.uy, m.uy, __fmul_rn(m.ux, m.ux)));
+  m.a = __fmul_rn(-1.5f, usq);
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    m.kd[c] = __fmul_rn(k.kw[c], dr);
+    m.kr[c] = __fadd_rn(k.kw[c], m.kd[c]);
+  }
+  return m;
+}
+
+// c_q.u: the first non-zero component, plus the second one if any.
+__device__ __forceinline__ float cdotu(int q, const Mom16& m) {
+  const int cx = cxq(q), cy = cyq(q), cz = czq(q);
+  float cu = 0.0f;
+  bool first = true;
+  if (cx != 0) { cu = cx > 0 ? m.ux : -m.ux; first = false; }
+  if (cy != 0) { const float t = cy > 0 ? m.uy : -m.uy; cu = first ? t : __fadd_rn(cu, t); first = false; }
+  if (cz != 0) { const float t = cz > 0 ? m.uz : -m.uz; cu = first ? t : __fadd_rn(cu, t); }
+  return cu;
+}
+
+// Post-collision scaled values of the pair (q, opp q), q in 0..8.
+__device__ __forceinline__ void pair16(int q, float yq, float yo, const Mom16& m, float om1, float& oq, float& oo) {
+  const int c = wclass(q);
+  const float cu = cdotu(q, m);
+  const float q2 = __fmaf_rn(__fmul_rn(4.5f, cu), cu, m.a);
+  const float pp = __fmaf_rn(3.0f, cu, q2);
+  const float pm = __fmaf_rn(-3.0f, cu, q2);
+  oq = __fmaf_rn(m.kr[c], pp, __fmaf_rn(om1, yq, m.kd[c]));
+  oo = __fmaf_rn(m.kr[c], pm, __fmaf_rn(om1, yo, m.kd[c]));
+}
+
+// Rest population (cu = 0, P = a).
+__device__ __forceinline__ float rest16(float y, const Mom16& m, float om1) {
+  return __fmaf_rn(m.kr[0], m.a, __fmaf_rn(om1, y, m.kd[0]));
+}
+
 struct F16 {
   using S = __half; using R = float; using V = Ex<float>;
   static constexpr int id = 2;
   // inv and scale are exact powers of two: the multiply only moves the exponent
   __device__ static __forceinline__ R dec(S s, R inv) { return __fmul_rn(__half2float(s), inv); }
   __device__ static __forceinline__ S enc(R r, R scale) { return __float2half_rn(__fmul_rn(r, scale)); }
+  __device__ static __forceinline__ void cell(S (&s)[Q], const StepK& k) {
+    float y[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) y[q] = __half2float(s[q]);
+    const Mom16 m = moments16(y, k);
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+      float a, b;
+      pair16(q, y[q], y[oppq(q)], m, k.om1, a, b);
+      s[q] = __float2half_rn(a);
+      s[oppq(q)] = __float2half_rn(b);
+    }
+    s[Q - 1] = __float2half_rn(rest16(y[Q - 1], m, k.om1));
+  }
 };
 
 // ----------------------------------------------------------------- geometry

@@ -1,0 +1,116 @@
+"""Accuracy of the FP32 and FP16 storage forms against FP64 on decaying HIT.
+
+    python -m bgk3d_hit_b200.precision_study [--size 512] [--steps 5000] [--every 100]
+        [--k0 6] [--tau 0.503] [--scheme two_lattice] [--out results.json]
+
+Runs the same seeded HIT initial condition (random-phase solenoidal field,
+E(k) ~ k^4 exp(-2 (k/k0)^2), u_rms = 0.03) in the three storage forms side by
+side on one GPU, through the public API, and reports against the FP64 run:
+- E(t): mean kinetic energy 0.5|u|^2 of the local velocity (diagno column),
+- eps(t): strain-rate dissipation 2 nu <S:S>, S = -3 omega Pi_neq / (2 rho),
+- E(k): shell spectrum of the final velocity field,
+as maximum relative errors over the run (E, eps) and over the shells that hold
+at least 1e-6 of the peak energy (E(k)). Prints one JSON object.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import time
+
+import numpy as np
+
+from .hit import hit_velocity
+from .solver import BGK3D
+
+FORMS = ("fp64", "fp32", "fp16")
+
+
+def run(size=512, steps=5000, every=100, k0=6.0, tau=0.503, u_rms=0.03, seed=1234, scheme="two_lattice",
+        forms=FORMS, device=0):
+    svisc = (tau - 0.5) / 3.0
+    t0 = time.time()
+    u, v, w = hit_velocity(size, k0, u_rms, seed)
+    t_ic = time.time() - t0
+    boxes = {}
+    for f in forms:
+        b = BGK3D(size, svisc=svisc, u0=u_rms, precision=f, scheme=scheme, icheck=every, device=device)
+        b.init_velocity(u, v, w)
+        boxes[f] = b
+    del u, v, w
+    series = {f: {"step": [], "E": [], "eps": [], "diss": [], "rho": []} for f in forms}
+
+    def record(it):
+        for f, b in boxes.items():
+            d = b.diagnostic(it) if it > 0 else None
+            if it == 0:
+                dg = b.diagno(0)
+                ds = b.dissipation(0)
+                d = {"ke_mean": dg[4], "rho_mean": dg[0], "diss": ds[2], "eps_strain": float("nan")}
+            if d is None:
+                continue
+            s = series[f]
+            s["step"].append(it)
+            s["E"].append(d["ke_mean"])
+            s["eps"].append(d["eps_strain"])
+            s["diss"].append(d["diss"])
+            s["rho"].append(d["rho_mean"])
+
+    record(0)
+    t0 = time.time()
+    for it in range(1, steps + 1):
+        for b in boxes.values():
+            b.boundaries(it)
+            b.col_MC(it)
+        if it % every == 0 or it == steps:
+            record(it)
+    t_run = time.time() - t0
+    nb = size // 2 + 1
+    spec = {f: b.spectrum(nb) for f, b in boxes.items()}
+    for b in boxes.values():
+        b.close()
+
+    ref = series["fp64"] if "fp64" in series else None
+    out = {"config": {"size": size, "steps": steps, "every": every, "k0": k0, "tau": tau, "u_rms": u_rms,
+                      "seed": seed, "scheme": scheme},
+           "seconds": {"initial_condition": t_ic, "run": t_run}, "forms": {}}
+    for f in forms:
+        s = series[f]
+        rec = {"E_final": s["E"][-1], "E_initial": s["E"][0], "eps_final": s["eps"][-1]}
+        if ref is not None and f != "fp64":
+            E, Er = np.array(s["E"]), np.array(ref["E"])
+            ep, epr = np.array(s["eps"][1:]), np.array(ref["eps"][1:])
+            rec["E_max_rel_err"] = float(np.max(np.abs(E - Er) / np.abs(Er)))
+            rec["eps_max_rel_err"] = float(np.max(np.abs(ep - epr) / np.abs(epr)))
+            rec["diss_max_rel_err"] = float(np.max(np.abs(np.array(s["diss"][1:]) - np.array(ref["diss"][1:])) /
+                                                np.abs(np.array(ref["diss"][1:]))))
+            ek, ekr = spec[f], spec["fp64"]
+            mask = ekr >= 1e-6 * ekr.max()
+            rec["Ek_max_rel_err"] = float(np.max(np.abs(ek[mask] - ekr[mask]) / ekr[mask]))
+            rec["Ek_shells"] = int(mask.sum())
+            rec["rho_mean_drift"] = float(abs(s["rho"][-1] - s["rho"][0]))
+        out["forms"][f] = rec
+    out["series"] = {f: {k: list(map(float, v)) for k, v in series[f].items()} for f in forms}
+    out["spectrum"] = {f: list(map(float, spec[f])) for f in forms}
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--size", type=int, default=512)
+    ap.add_argument("--steps", type=int, default=5000)
+    ap.add_argument("--every", type=int, default=100)
+    ap.add_argument("--k0", type=float, default=6.0)
+    ap.add_argument("--tau", type=float, default=0.503)
+    ap.add_argument("--scheme", default="two_lattice")
+    ap.add_argument("--out", default=None, help="write the full series and spectra here (JSON)")
+    a = ap.parse_args()
+    res = run(a.size, a.steps, a.every, a.k0, a.tau, scheme=a.scheme)
+    if a.out:
+        with open(a.out, "w") as f:
+            json.dump(res, f)
+    print(json.dumps({"config": res["config"], "seconds": res["seconds"], "forms": res["forms"]}))
+
+
+if __name__ == "__main__":
+    main()

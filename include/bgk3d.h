@@ -80,6 +80,11 @@ typedef struct {
   int use_omega;       /* 1: use `omega` below instead of the svisc formula */
   double omega;        /* collision frequency override (e.g. 0 = pure streaming) */
   int extras;          /* 1: bgk_diagnostic also computes enstrophy */
+  int kernel;          /* stream-collide kernel: 0 automatic, 1 one cell per thread,
+                          2 / 4 two / four cells per thread (FP16 two-lattice), 8 row
+                          pipeline with TMA bulk copies into shared memory (rows up to
+                          about 5 KB); boxes a kernel does not fit use 1. All give
+                          identical results. */
 } bgk_params;
 
 /* Diagnostics of one step, in FP64. */
@@ -207,6 +212,13 @@ int bgk_shift3(const void* in1, const void* in2, const void* in3, void* out1, vo
 int bgk_diagnostics_noalloc(const void* const* pops19, int lx, int ly, int lz, int pitch_x, int precision,
                             double svisc, double omega, double u0, double fp16_scale, int mode, int itime,
                             bgk_diag* out, void* stream);
+
+/* Test hook for the failure path of the row-pipelined kernel (params.kernel
+   = 8): during the next bgk_col_mc its first CTA waits on a barrier that
+   nothing arms; the bounded wait runs out, the step is abandoned and the next
+   synchronising call returns BGK_ERR_CUDA. The context stays usable after a
+   new bgk_init_* or bgk_put_populations. Faults nothing. */
+int bgk_debug_stall_next_step(bgk_ctx* ctx);
 
 const char* bgk_strerror(int code);
 /* Message of the last error on this thread. */

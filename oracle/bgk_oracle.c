@@ -9,7 +9,9 @@
  *   _f64  double storage, double arithmetic  (reference DOUBLE_P build)
  *   _f32  float storage, float arithmetic    (reference default build)
  *   _f16  binary16 storage of scale*(f - w), float arithmetic (no reference
- *         counterpart; the reference stops on HALF_P, SRC/precision.F90:40-43)
+ *         counterpart; the reference stops on HALF_P, SRC/precision.F90:40-43);
+ *         its collision is the fused-multiply-add form defined in
+ *         fast16_cell, shared operation for operation with the CUDA kernels
  *
  * Parity unpinned: the reference has no tests or golden vectors, and its
  * Fortran/MPI build cannot be compiled here. Only tests/, the smoke check and
@@ -59,6 +61,7 @@
 #undef ENC
 #undef DEC
 
+#define FAST16
 #define SUF _f16
 #define STOR _Float16
 #define REAL float
@@ -67,6 +70,7 @@
 #define ENC(L, x) ((_Float16)((x) * (L)->scale))
 #define DEC(L, s) ((float)(s) * (L)->inv_scale)
 #include "bgk_oracle_impl.h"
+#undef FAST16
 #undef SUF
 #undef STOR
 #undef REAL

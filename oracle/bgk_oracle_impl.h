@@ -289,22 +289,97 @@ double FN(orc_omega)(double svisc) {
     return (double)o;
 }
 
+#ifdef FAST16
+/* Collision of the FP16 form (no reference counterpart: the reference stops
+   on HALF_P, SRC/precision.F90:40-43). It works on the scaled stored values
+   y = scale*(f - w) as floats, keeps dr = sum(f - w) apart from 1, treats each
+   pair of opposite directions (q, opp q), q = 0..8, together and uses fused
+   multiply-adds (C fmaf, correctly rounded):
+     dr = sum(y)*inv, u = j(y)*(inv/(1 + dr)), a = -1.5|u|^2,
+     kd = K*dr, kr = K + kd with K = omega*scale*w (per weight class),
+     Q2 = fmaf(4.5*cu, cu, a), P(+-) = fmaf(+-3, cu, Q2),
+     y' = fmaf(kr, P, fmaf(1 - omega, y, kd)).
+   The sums are grouped as written; this is the definition the CUDA kernels
+   follow operation for operation. */
+static inline float FN(cdotu16)(int q, float ux, float uy, float uz) {
+    const int cx = FN(CX)[q], cy = FN(CY)[q], cz = FN(CZ)[q];
+    float cu = 0.0f;
+    int first = 1;
+    if (cx != 0) { cu = cx > 0 ? ux : -ux; first = 0; }
+    if (cy != 0) { float t = cy > 0 ? uy : -uy; cu = first ? t : cu + t; first = 0; }
+    if (cz != 0) { float t = cz > 0 ? uz : -uz; cu = first ? t : cu + t; }
+    return cu;
+}
+
+static void FN(fast16_cell)(const float *y, float *out, float inv, float om1, const float kw[3]) {
+    static const int opp[9] = {11, 12, 9, 10, 13, 14, 15, 16, 17};
+    static const int wcls[19] = {2,2,2,2,1,1,2,1,2,2,2,2,2,1,1,2,1,2,0};
+    const float sp = ((y[0] + y[1]) + (y[2] + y[3])) + y[4];
+    const float sm = ((y[9] + y[10]) + (y[11] + y[12])) + y[13];
+    const float s0 = (((y[5] + y[6]) + (y[7] + y[8])) + ((y[14] + y[15]) + (y[16] + y[17]))) + y[18];
+    const float sum = (sp + sm) + s0;
+    const float jx = sp - sm;
+    const float jyp = ((y[2] + y[6]) + (y[7] + y[8])) + y[11];
+    const float jym = ((y[0] + y[9]) + (y[15] + y[16])) + y[17];
+    const float jzp = ((y[3] + y[5]) + (y[6] + y[12])) + y[17];
+    const float jzm = ((y[1] + y[8]) + (y[10] + y[14])) + y[15];
+    const float dr = sum * inv;
+    const float r = inv / (1.0f + dr);
+    const float ux = jx * r, uy = (jyp - jym) * r, uz = (jzp - jzm) * r;
+    const float usq = fmaf(uz, uz, fmaf(uy, uy, ux * ux));
+    const float a = -1.5f * usq;
+    float kd[3], kr[3];
+    for (int c = 0; c < 3; ++c) { kd[c] = kw[c] * dr; kr[c] = kw[c] + kd[c]; }
+    for (int q = 0; q < 9; ++q) {
+        const int c = wcls[q], o = opp[q];
+        const float cu = FN(cdotu16)(q, ux, uy, uz);
+        const float q2 = fmaf(4.5f * cu, cu, a);
+        const float pp = fmaf(3.0f, cu, q2), pm = fmaf(-3.0f, cu, q2);
+        out[q] = fmaf(kr[c], pp, fmaf(om1, y[q], kd[c]));
+        out[o] = fmaf(kr[c], pm, fmaf(om1, y[o], kd[c]));
+    }
+    out[18] = fmaf(kr[0], a, fmaf(om1, y[18], kd[0]));
+}
+#endif
+
 /* One fused pull-stream + BGK collide over the interior followed by the swap
    of pops 01..18, SRC/col_MC.F90:98-421. omega is passed in REAL precision.
    periodic selects ghost reads (reference) or modulo indexing. */
 void FN(orc_col_mc_omega)(LAT *L, double omegad, int periodic) {
     const REAL omega = (REAL)omegad;
     const long l = L->l, m = L->m, n = L->n;
+#ifdef FAST16
+    const float inv = (float)L->inv_scale, om1 = 1.0f - (float)omega;
+    const double wd[3] = {1.0 / 3.0, 1.0 / 18.0, 1.0 / 36.0};
+    float kw[3];
+    for (int c = 0; c < 3; ++c) kw[c] = (float)((double)(float)omega * (double)L->scale * wd[c]);
+#endif
 #pragma omp parallel for schedule(static)
     for (long k = 1; k <= n; ++k)
         for (long j = 1; j <= m; ++j)
             for (long i = 1; i <= l; ++i) {
+                long g = FN(gidx)(L, i, j, k);
+#ifdef FAST16
+                float y[19], out[19];
+                for (int q = 0; q < 19; ++q) {
+                    long si = i - FN(CX)[q], sj = j - FN(CY)[q], sk = k - FN(CZ)[q];
+                    if (periodic) {
+                        si = (si - 1 + l) % l + 1;
+                        sj = (sj - 1 + m) % m + 1;
+                        sk = (sk - 1 + n) % n + 1;
+                    }
+                    y[q] = (float)L->a[q][FN(gidx)(L, si, sj, sk)];
+                }
+                FN(fast16_cell)(y, out, inv, om1, kw);
+                for (int q = 0; q < 18; ++q) L->b[q][g] = (STOR)out[q];
+                L->a[18][g] = (STOR)out[18];
+#else
                 REAL x[19], e[19], ux, uy, uz;
                 FN(pull)(L, L->a, i, j, k, periodic, x);
                 (void)FN(equilibrium)(x, e, &ux, &uy, &uz);
-                long g = FN(gidx)(L, i, j, k);
                 for (int q = 0; q < 18; ++q) L->b[q][g] = ENC(L, x[q] - omega * (x[q] - e[q]));
                 L->a[18][g] = ENC(L, x[18] - omega * (x[18] - e[18]));
+#endif
             }
     for (int q = 0; q < 18; ++q) {
         STOR *c = L->a[q]; L->a[q] = L->b[q]; L->b[q] = c;

@@ -71,6 +71,7 @@ def test_defaults(bgk):
     dict(lx=0), dict(lz=-3), dict(precision=7), dict(scheme=2), dict(mode=5), dict(icheck=0),
     dict(svisc=0.0), dict(svisc=-1.0), dict(svisc=float("nan")), dict(use_omega=1, omega=2.5),
     dict(fp16_scale=3.0), dict(fp16_scale=-2.0), dict(u0=float("inf")), dict(lx=4096, ly=4096, lz=4096),
+    dict(kernel=3), dict(kernel=-1), dict(kernel=16),
 ])
 def test_create_rejects_bad_parameters_before_touching_a_device(bgk, bad):
     lib = bgk.load()

@@ -48,6 +48,59 @@ def test_two_lattice_bitexact_vs_oracle(bgk, oracle_mod, form, shape):
     box.close()
 
 
+@pytest.mark.parametrize("kernel", [1, 2, 4])
+@pytest.mark.parametrize("shape", [(64, 64, 64), (32, 16, 8), (8, 8, 8), (256, 4, 4), (128, 6, 5), (24, 8, 6)])
+def test_fp16_kernel_variants_bitexact(bgk, oracle_mod, kernel, shape):
+    """The one-, two- and four-cells-per-thread FP16 kernels (warp-shuffle
+    x-shifts, cross-warp loads when a row spans several warps, fallback where a
+    box does not fit) give the oracle's bits."""
+    orc, box = make_pair(bgk, oracle_mod, shape, "fp16", kernel=kernel)
+    for it in range(1, 6):
+        orc.step(0.01, periodic=True)
+        box.col_MC(it)
+    assert same_bits(box.populations(), orc.get_pops())
+    box.close()
+
+
+@pytest.mark.parametrize("form", ["fp64", "fp32", "fp16"])
+@pytest.mark.parametrize("scheme", ["two_lattice", "aa"])
+@pytest.mark.parametrize("shape", [(5, 7, 9), (64, 16, 8), (33, 20, 7), (256, 3, 2)])
+def test_row_pipeline_kernel_bitexact(bgk, oracle_mod, form, scheme, shape):
+    """The TMA row-pipelined kernel (kernel 8) gives the oracle's bits in both
+    schemes, over steps of both AA parities."""
+    orc, box = make_pair(bgk, oracle_mod, shape, form, scheme=scheme, kernel=8)
+    for it in range(1, 8):
+        orc.step(0.01, periodic=True)
+        box.col_MC(it)
+        if it in (1, 2, 7):
+            assert same_bits(box.populations(), orc.get_pops()), f"after {it} steps"
+    box.close()
+
+
+def test_row_pipeline_bounded_wait_reports_and_recovers(bgk, oracle_mod):
+    """A wait that runs out (injected: a barrier nothing arms) abandons the
+    step, is reported at the next synchronisation, and the context recovers
+    after a new initialisation. No fault is involved."""
+    B = bgk
+    orc, box = make_pair(bgk, oracle_mod, (64, 16, 8), "fp64", kernel=8)
+    lib = B.load()
+    assert lib.bgk_debug_stall_next_step(box._h) == 0
+    box.col_MC(1)
+    with pytest.raises(B.BgkError) as e:
+        box.synchronize()
+    assert e.value.code == B._abi.BGK_ERR_CUDA and "gave up" in str(e.value)
+    box.set_populations(orc.get_pops())
+    orc.step(0.01, periodic=True)
+    box.col_MC(1)
+    box.synchronize()
+    assert same_bits(box.populations(), orc.get_pops())
+    box.close()
+    plain = B.BGK3D(8, kernel=1)
+    with pytest.raises(B.BgkError):
+        B._abi.check(lib.bgk_debug_stall_next_step(plain._h), "stall")
+    plain.close()
+
+
 @pytest.mark.parametrize("form", ["fp64", "fp32", "fp16"])
 @pytest.mark.parametrize("shape", [(5, 7, 9), (32, 16, 8)])
 def test_aa_pattern_bitexact_vs_oracle(bgk, oracle_mod, form, shape):

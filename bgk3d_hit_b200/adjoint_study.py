@@ -1,0 +1,119 @@
+"""Checks and costs of the discrete adjoint on decaying HIT.
+
+    python -m bgk3d_hit_b200.adjoint_study [--size 128] [--steps 1000] [--ckpt 32]
+        [--tau 0.51] [--k0 4] [--dirs 64] [--h 1e-6] [--precision fp64]
+
+Initial velocity: seeded HIT field (seed 1234, E(k) ~ k^4 exp(-2 (k/k0)^2),
+u_rms = 0.03); target u_tgt: the same generator with a second seed (4321).
+Loss = 0.5 mean |u(T) - u_tgt|^2. Reports, as one JSON object:
+- fd: the relative error of <grad, d> against central differences
+  (L(u0 + h d) - L(u0 - h d)) / 2h over `dirs` seeded random unit directions d
+  (max and median), and the same for tau;
+- tangent: the relative difference between <grad, d> + grad_tau dtau and the
+  tangent-linear derivative along (d, dtau) for a few directions;
+- cost: wall time of the adjoint call (forward with checkpoints, recomputation,
+  backward) over the wall time of a forward-only call of the same length.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import time
+
+import numpy as np
+
+from .hit import hit_velocity
+from .solver import BGK3D
+
+DP = C.POINTER(C.c_double)
+
+
+def _p(a):
+    return a.ctypes.data_as(DP)
+
+
+def _adj(box, u0, ut, T, K, grads):
+    n = box.ncell
+    loss, gt = C.c_double(), C.c_double()
+    g = np.zeros(3 * n) if grads else None
+    rc = box._lib.bgk_adjoint(box._h, _p(u0[0]), _p(u0[1]), _p(u0[2]), _p(ut[0]), _p(ut[1]), _p(ut[2]), T, K,
+                              C.byref(loss), _p(g) if grads else None, C.byref(gt) if grads else None)
+    if rc:
+        raise RuntimeError(box._lib.bgk_last_error().decode())
+    return loss.value, g, gt.value
+
+
+def run(size=128, steps=1000, ckpt=32, tau=0.51, k0=4.0, u_rms=0.03, dirs=64, h=1e-6, precision="fp64", ntan=4):
+    svisc = (tau - 0.5) / 3.0
+    u0 = [np.ascontiguousarray(a) for a in hit_velocity(size, k0, u_rms, 1234)]
+    ut = [np.ascontiguousarray(a) for a in hit_velocity(size, k0, u_rms, 4321)]
+    box = BGK3D(size, svisc=svisc, u0=u_rms, precision=precision)
+    tau_used = 1.0 / box.omega
+    # cost: forward-only and full adjoint, each timed after one warm-up call
+    _adj(box, u0, ut, steps, ckpt, False)
+    t0 = time.perf_counter()
+    loss, _, _ = _adj(box, u0, ut, steps, ckpt, False)
+    t_fwd = time.perf_counter() - t0
+    _adj(box, u0, ut, steps, ckpt, True)
+    t0 = time.perf_counter()
+    loss2, g, gtau = _adj(box, u0, ut, steps, ckpt, True)
+    t_adj = time.perf_counter() - t0
+    rng = np.random.default_rng(2024)
+    errs = []
+    for _ in range(dirs):
+        d = rng.standard_normal((3,) + u0[0].shape)
+        d /= np.linalg.norm(d)
+        lp = _adj(box, [a + h * b for a, b in zip(u0, d)], ut, steps, ckpt, False)[0]
+        lm = _adj(box, [a - h * b for a, b in zip(u0, d)], ut, steps, ckpt, False)[0]
+        fd = (lp - lm) / (2 * h)
+        ad = float(np.dot(g, d.reshape(-1)))
+        errs.append(abs(ad - fd) / max(abs(fd), 1e-300))
+    # tau by central differences of boxes with omega = 1/(tau +- h)
+    lt = []
+    for s in (1, -1):
+        b2 = BGK3D(size, omega=1.0 / (tau_used + s * h), precision=precision, u0=u_rms)
+        lt.append(_adj(b2, u0, ut, steps, ckpt, False)[0])
+        b2.close()
+    fd_tau = (lt[0] - lt[1]) / (2 * h)
+    # tangent-linear checks
+    tan_errs = []
+    for m in range(ntan):
+        d = rng.standard_normal((3,) + u0[0].shape)
+        dtau = float(rng.standard_normal())
+        lo, dl = C.c_double(), C.c_double()
+        dd = [np.ascontiguousarray(x) for x in d]
+        rc = box._lib.bgk_tangent(box._h, _p(u0[0]), _p(u0[1]), _p(u0[2]), _p(dd[0]), _p(dd[1]), _p(dd[2]), dtau,
+                                  _p(ut[0]), _p(ut[1]), _p(ut[2]), steps, C.byref(lo), C.byref(dl))
+        if rc:
+            raise RuntimeError(box._lib.bgk_last_error().decode())
+        pred = float(np.dot(g, d.reshape(-1))) + gtau * dtau
+        tan_errs.append(abs(pred - dl.value) / abs(dl.value))
+    box.close()
+    return {
+        "config": {"size": size, "steps": steps, "ckpt_every": ckpt, "tau": tau_used, "k0": k0, "u_rms": u_rms,
+                   "precision": precision, "h": h, "directions": dirs},
+        "loss": loss, "loss_in_adjoint_call": loss2, "grad_tau": gtau, "fd_grad_tau": fd_tau,
+        "fd": {"max_rel_err": float(np.max(errs)), "median_rel_err": float(np.median(errs)),
+               "tau_rel_err": abs(gtau - fd_tau) / abs(fd_tau)},
+        "tangent": {"max_rel_err": float(np.max(tan_errs)), "directions": ntan},
+        "cost": {"forward_s": t_fwd, "adjoint_s": t_adj, "adjoint_over_forward": t_adj / t_fwd},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--size", type=int, default=128)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--ckpt", type=int, default=32)
+    ap.add_argument("--tau", type=float, default=0.51)
+    ap.add_argument("--k0", type=float, default=4.0)
+    ap.add_argument("--dirs", type=int, default=64)
+    ap.add_argument("--h", type=float, default=1e-6)
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
+    a = ap.parse_args()
+    print(json.dumps(run(a.size, a.steps, a.ckpt, a.tau, a.k0, dirs=a.dirs, h=a.h, precision=a.precision)))
+
+
+if __name__ == "__main__":
+    main()

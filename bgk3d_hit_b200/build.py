@@ -19,8 +19,8 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 OUT = os.path.join(HERE, "libbgk3d.so")
-SOURCES = ["kernels.cu", "rows.cu", "bgk_abi.cu", "noalloc.cu"]
-HEADERS = ["lattice.cuh", "kernels.h"]
+SOURCES = ["kernels.cu", "rows.cu", "adjoint.cu", "bgk_abi.cu", "noalloc.cu"]
+HEADERS = ["lattice.cuh", "kernels.h", "reduce.cuh"]
 ARCH = "-gencode=arch=compute_100a,code=sm_100a"
 
 

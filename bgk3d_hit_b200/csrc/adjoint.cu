@@ -1,0 +1,329 @@
+// Discrete adjoint and tangent-linear model of the fused stream-collide step
+// (no reference counterpart). For one cell with pulled deviations g,
+// rho = 1 + sum g, u = j/rho, P_p = 3 c_p.u + 4.5 (c_p.u)^2 - 1.5 |u|^2,
+// e_p = w_p rho (1 + P_p) - w_p and f_p = g_p - omega (g_p - e_p):
+//
+//   adjoint   mu_q = (1 - omega) lam_q + omega (A - B.u + B.c_q),
+//             A = sum_p w_p lam_p (1 + P_p),
+//             B_a = 3 sum_p w_p lam_p c_pa (1 + 3 c_p.u) - 3 u_a sum_p w_p lam_p,
+//             and reverse streaming lam_t,q(x - c_q) = mu_q(x);
+//   dL/domega = sum over steps and cells of -lam.(g - e);
+//   tangent   df_p = (1 - omega) dg_p + omega de_p + (e_p - g_p) domega,
+//             de_p = w_p [(1 + P_p) drho + rho (3 (c_p.du)(1 + 3 c_p.u) - 3 u.du)],
+//             drho = sum dg, du = (dj - u drho)/rho.
+// The initial state f0_q = w_q P_q(u0) (rho = 1, the equilibrium of
+// bgk_init_velocity) gives dL/du0 = B(lam_0, u0). The forward arithmetic of
+// the step (rho, u, e) is the library's own (equilibrium<V>), so the adjoint
+// differentiates exactly the map that bgk_col_mc applies.
+//
+// Kernels run a fixed grid (DIAG_BLOCKS x DIAG_THREADS) striding over the
+// cells, and accumulate their sums into one compensated pair per block, so
+// repeated runs give identical bits.
+#include "kernels.h"
+#include "reduce.cuh"
+
+namespace bgk {
+
+namespace {
+
+__device__ __forceinline__ int wrapa(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
+
+// Adds the block's compensated sum v into its running pair acc[2*blk].
+__device__ __forceinline__ void acc_block(KS v, KS* sh, double* acc) {
+  const KS r = block_reduce(v, sh);
+  if (threadIdx.x == 0) {
+    KS a{acc[2 * blockIdx.x], acc[2 * blockIdx.x + 1]};
+    kcomb(a, r);
+    acc[2 * blockIdx.x] = a.s;
+    acc[2 * blockIdx.x + 1] = a.c;
+  }
+}
+
+template <class R>
+__device__ __forceinline__ R cdot(int q, R ux, R uy, R uz) {
+  return (R)cxq(q) * ux + (R)cyq(q) * uy + (R)czq(q) * uz;
+}
+
+template <class R>
+__device__ __forceinline__ R wq(int q) {
+  return wclass(q) == 0 ? (R)(1.0 / 3.0) : (wclass(q) == 1 ? (R)(1.0 / 18.0) : (R)(1.0 / 36.0));
+}
+
+template <class F>
+__global__ void __launch_bounds__(DIAG_THREADS) k_adj_terminal(Pops<const typename F::S> f, Geo g,
+                                                               const double* __restrict__ ut, Pops<typename F::S> lam,
+                                                               double* acc) {
+  using S = typename F::S; using V = typename F::V; using N = Num<V>;
+  __shared__ KS sh[DIAG_THREADS];
+  KS loss = {0.0, 0.0};
+  const long long n = (long long)g.nx * g.ny * g.nz;
+  const double invn = 1.0 / (double)n;
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(c % g.nx), j = (int)((c / g.nx) % g.ny), k = (int)(c / ((long long)g.nx * g.ny));
+    const long long o = i + (long long)g.sx * (j + (long long)g.ny * k);
+    V x[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) x[q] = V{f.p[q][o]};
+    V e[Q], vx, vy, vz;
+    const V rho = equilibrium<V>(x, e, vx, vy, vz);  // moments in the forward's order
+    const double u[3] = {(double)N::raw(vx), (double)N::raw(vy), (double)N::raw(vz)};
+    const double d[3] = {u[0] - ut[c], u[1] - ut[n + c], u[2] - ut[2 * n + c]};
+    kadd(loss, 0.5 * (d[0] * d[0] + d[1] * d[1] + d[2] * d[2]));
+    const double r = invn / (double)N::raw(rho);
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      const double l = r * (d[0] * (cxq(q) - u[0]) + d[1] * (cyq(q) - u[1]) + d[2] * (czq(q) - u[2]));
+      lam.p[q][o] = (S)l;
+    }
+  }
+  acc_block(loss, sh, acc);
+}
+
+template <class F>
+__global__ void __launch_bounds__(DIAG_THREADS) k_adj_step(Pops<const typename F::S> ft, Pops<const typename F::S> lin,
+                                                           Pops<typename F::S> lout, Geo g, typename F::R omega,
+                                                           double* acc) {
+  using S = typename F::S; using R = typename F::R; using V = typename F::V; using N = Num<V>;
+  __shared__ KS sh[DIAG_THREADS];
+  KS dom = {0.0, 0.0};
+  const long long n = (long long)g.nx * g.ny * g.nz;
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(c % g.nx), j = (int)((c / g.nx) % g.ny), k = (int)(c / ((long long)g.nx * g.ny));
+    const long long o = i + (long long)g.sx * (j + (long long)g.ny * k);
+    long long off[Q];
+    V x[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      const int ii = wrapa(i - cxq(q), g.nx), jj = wrapa(j - cyq(q), g.ny), kk = wrapa(k - czq(q), g.nz);
+      off[q] = ii + (long long)g.sx * (jj + (long long)g.ny * kk);
+      x[q] = V{ft.p[q][off[q]]};
+    }
+    V e[Q], vx, vy, vz;
+    (void)equilibrium<V>(x, e, vx, vy, vz);
+    const R ux = N::raw(vx), uy = N::raw(vy), uz = N::raw(vz);
+    const R usq = ux * ux + uy * uy + uz * uz;
+    R A = 0, L0 = 0, Lx = 0, Ly = 0, Lz = 0;
+    double dw = 0.0;
+    R lam[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      lam[q] = (R)lin.p[q][o];
+      const R cu = cdot<R>(q, ux, uy, uz);
+      const R P = (R)3 * cu + (R)4.5 * cu * cu - (R)1.5 * usq;
+      const R wl = wq<R>(q) * lam[q];
+      A += wl * ((R)1 + P);
+      L0 += wl;
+      const R t = wl * ((R)1 + (R)3 * cu);
+      Lx += t * (R)cxq(q);
+      Ly += t * (R)cyq(q);
+      Lz += t * (R)czq(q);
+      dw -= (double)lam[q] * ((double)N::raw(x[q]) - (double)N::raw(e[q]));
+    }
+    kadd(dom, dw);
+    const R Bx = (R)3 * Lx - (R)3 * ux * L0, By = (R)3 * Ly - (R)3 * uy * L0, Bz = (R)3 * Lz - (R)3 * uz * L0;
+    const R G = A - (Bx * ux + By * uy + Bz * uz);
+    const R om1 = (R)1 - omega;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      const R mu = om1 * lam[q] + omega * (G + cdot<R>(q, Bx, By, Bz));
+      lout.p[q][off[q]] = (S)mu;  // reverse streaming: lam_t,q(x - c_q) = mu_q(x)
+    }
+  }
+  acc_block(dom, sh, acc);
+}
+
+template <class F>
+__global__ void __launch_bounds__(DIAG_THREADS) k_adj_grad_u0(Pops<const typename F::S> lam, Geo g,
+                                                              const double* __restrict__ u0, double* grad) {
+  const long long n = (long long)g.nx * g.ny * g.nz;
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(c % g.nx), j = (int)((c / g.nx) % g.ny), k = (int)(c / ((long long)g.nx * g.ny));
+    const long long o = i + (long long)g.sx * (j + (long long)g.ny * k);
+    const double ux = u0[c], uy = u0[n + c], uz = u0[2 * n + c];
+    double L0 = 0, Lx = 0, Ly = 0, Lz = 0;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      const double wl = wq<double>(q) * (double)lam.p[q][o];
+      const double t = wl * (1.0 + 3.0 * cdot<double>(q, ux, uy, uz));
+      L0 += wl;
+      Lx += t * cxq(q);
+      Ly += t * cyq(q);
+      Lz += t * czq(q);
+    }
+    grad[c] = 3.0 * Lx - 3.0 * ux * L0;
+    grad[n + c] = 3.0 * Ly - 3.0 * uy * L0;
+    grad[2 * n + c] = 3.0 * Lz - 3.0 * uz * L0;
+  }
+}
+
+template <class F>
+__global__ void __launch_bounds__(DIAG_THREADS) k_tan_init(Pops<typename F::S> df, Geo g,
+                                                           const double* __restrict__ u0,
+                                                           const double* __restrict__ du0) {
+  using S = typename F::S;
+  const long long n = (long long)g.nx * g.ny * g.nz;
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(c % g.nx), j = (int)((c / g.nx) % g.ny), k = (int)(c / ((long long)g.nx * g.ny));
+    const long long o = i + (long long)g.sx * (j + (long long)g.ny * k);
+    const double ux = u0[c], uy = u0[n + c], uz = u0[2 * n + c];
+    const double dx = du0[c], dy = du0[n + c], dz = du0[2 * n + c];
+    const double udu = ux * dx + uy * dy + uz * dz;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      const double cu = cdot<double>(q, ux, uy, uz), cdu = cdot<double>(q, dx, dy, dz);
+      df.p[q][o] = (S)(wq<double>(q) * (3.0 * cdu * (1.0 + 3.0 * cu) - 3.0 * udu));
+    }
+  }
+}
+
+template <class F>
+__global__ void __launch_bounds__(DIAG_THREADS) k_tan_step(Pops<const typename F::S> f, Pops<const typename F::S> df,
+                                                           Pops<typename F::S> f2, Pops<typename F::S> df2, Geo g,
+                                                           typename F::R omega, typename F::R domega) {
+  using S = typename F::S; using R = typename F::R; using V = typename F::V; using N = Num<V>;
+  const long long n = (long long)g.nx * g.ny * g.nz;
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(c % g.nx), j = (int)((c / g.nx) % g.ny), k = (int)(c / ((long long)g.nx * g.ny));
+    const long long o = i + (long long)g.sx * (j + (long long)g.ny * k);
+    V x[Q];
+    R dx[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      const int ii = wrapa(i - cxq(q), g.nx), jj = wrapa(j - cyq(q), g.ny), kk = wrapa(k - czq(q), g.nz);
+      const long long off = ii + (long long)g.sx * (jj + (long long)g.ny * kk);
+      x[q] = V{f.p[q][off]};
+      dx[q] = (R)df.p[q][off];
+    }
+    V e[Q], vx, vy, vz;
+    const V rhov = equilibrium<V>(x, e, vx, vy, vz);
+    const R rho = N::raw(rhov), ux = N::raw(vx), uy = N::raw(vy), uz = N::raw(vz);
+    const R usq = ux * ux + uy * uy + uz * uz;
+    R drho = 0, djx = 0, djy = 0, djz = 0;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      drho += dx[q];
+      djx += (R)cxq(q) * dx[q];
+      djy += (R)cyq(q) * dx[q];
+      djz += (R)czq(q) * dx[q];
+    }
+    const R dux = (djx - ux * drho) / rho, duy = (djy - uy * drho) / rho, duz = (djz - uz * drho) / rho;
+    const R udu = ux * dux + uy * duy + uz * duz;
+    const R om1 = (R)1 - omega;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      const R cu = cdot<R>(q, ux, uy, uz), cdu = cdot<R>(q, dux, duy, duz);
+      const R P = (R)3 * cu + (R)4.5 * cu * cu - (R)1.5 * usq;
+      const R de = wq<R>(q) * (((R)1 + P) * drho + rho * ((R)3 * cdu * ((R)1 + (R)3 * cu) - (R)3 * udu));
+      df2.p[q][o] = (S)(om1 * dx[q] + omega * de + (N::raw(e[q]) - N::raw(x[q])) * domega);
+    }
+    collide<V>(x, V{omega});
+#pragma unroll
+    for (int q = 0; q < Q; ++q) f2.p[q][o] = N::raw(x[q]);
+  }
+}
+
+template <class F>
+__global__ void __launch_bounds__(DIAG_THREADS) k_tan_loss(Pops<const typename F::S> f, Pops<const typename F::S> df,
+                                                           Geo g, const double* __restrict__ ut, double* acc) {
+  using V = typename F::V; using N = Num<V>;
+  __shared__ KS sh[DIAG_THREADS];
+  KS dl = {0.0, 0.0};
+  const long long n = (long long)g.nx * g.ny * g.nz;
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(c % g.nx), j = (int)((c / g.nx) % g.ny), k = (int)(c / ((long long)g.nx * g.ny));
+    const long long o = i + (long long)g.sx * (j + (long long)g.ny * k);
+    V x[Q];
+    double drho = 0, djx = 0, djy = 0, djz = 0;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      x[q] = V{f.p[q][o]};
+      const double d = (double)df.p[q][o];
+      drho += d;
+      djx += cxq(q) * d;
+      djy += cyq(q) * d;
+      djz += czq(q) * d;
+    }
+    V e[Q], vx, vy, vz;
+    const double rho = (double)N::raw(equilibrium<V>(x, e, vx, vy, vz));
+    const double u[3] = {(double)N::raw(vx), (double)N::raw(vy), (double)N::raw(vz)};
+    const double du[3] = {(djx - u[0] * drho) / rho, (djy - u[1] * drho) / rho, (djz - u[2] * drho) / rho};
+    kadd(dl, (u[0] - ut[c]) * du[0] + (u[1] - ut[n + c]) * du[1] + (u[2] - ut[2 * n + c]) * du[2]);
+  }
+  acc_block(dl, sh, acc);
+}
+
+__global__ void __launch_bounds__(DIAG_THREADS) k_acc_total(const double* __restrict__ acc, double* total) {
+  __shared__ KS sh[DIAG_THREADS];
+  KS a = {0.0, 0.0};
+  for (int b = threadIdx.x; b < DIAG_BLOCKS; b += blockDim.x) kcomb(a, KS{acc[2 * b], acc[2 * b + 1]});
+  const KS r = block_reduce(a, sh);
+  if (threadIdx.x == 0) *total = __dadd_rn(r.s, r.c);
+}
+
+template <class S> Pops<S> pops(const Lattice& L) {
+  Pops<S> p;
+  for (int q = 0; q < Q; ++q) p.p[q] = (S*)L.p[q];
+  return p;
+}
+
+}  // namespace
+
+#define BGK_FORM_DISPATCH(L, CALL64, CALL32)      \
+  switch ((L).form) {                             \
+    case FORM_F64: CALL64; return cudaGetLastError(); \
+    case FORM_F32: CALL32; return cudaGetLastError(); \
+  }                                               \
+  return cudaErrorInvalidValue;
+
+cudaError_t launch_adj_terminal(const Lattice& f, const double* ut, const Lattice& lam, double* acc, cudaStream_t st) {
+  BGK_FORM_DISPATCH(f,
+      (k_adj_terminal<F64><<<DIAG_BLOCKS, DIAG_THREADS, 0, st>>>(pops<const double>(f), f.g, ut, pops<double>(lam), acc)),
+      (k_adj_terminal<F32><<<DIAG_BLOCKS, DIAG_THREADS, 0, st>>>(pops<const float>(f), f.g, ut, pops<float>(lam), acc)))
+}
+
+cudaError_t launch_adj_step(const Lattice& ft, const Lattice& lin, const Lattice& lout, double omega, double* acc,
+                            cudaStream_t st) {
+  BGK_FORM_DISPATCH(ft,
+      (k_adj_step<F64><<<DIAG_BLOCKS, DIAG_THREADS, 0, st>>>(pops<const double>(ft), pops<const double>(lin),
+                                                             pops<double>(lout), ft.g, omega, acc)),
+      (k_adj_step<F32><<<DIAG_BLOCKS, DIAG_THREADS, 0, st>>>(pops<const float>(ft), pops<const float>(lin),
+                                                             pops<float>(lout), ft.g, (float)omega, acc)))
+}
+
+cudaError_t launch_adj_grad_u0(const Lattice& lam0, const double* u0, double* grad, cudaStream_t st) {
+  BGK_FORM_DISPATCH(lam0,
+      (k_adj_grad_u0<F64><<<DIAG_BLOCKS, DIAG_THREADS, 0, st>>>(pops<const double>(lam0), lam0.g, u0, grad)),
+      (k_adj_grad_u0<F32><<<DIAG_BLOCKS, DIAG_THREADS, 0, st>>>(pops<const float>(lam0), lam0.g, u0, grad)))
+}
+
+cudaError_t launch_tan_init(const Lattice& df, const double* u0, const double* du0, cudaStream_t st) {
+  BGK_FORM_DISPATCH(df,
+      (k_tan_init<F64><<<DIAG_BLOCKS, DIAG_THREADS, 0, st>>>(pops<double>(df), df.g, u0, du0)),
+      (k_tan_init<F32><<<DIAG_BLOCKS, DIAG_THREADS, 0, st>>>(pops<float>(df), df.g, u0, du0)))
+}
+
+cudaError_t launch_tan_step(const Lattice& f, const Lattice& df, const Lattice& f2, const Lattice& df2, double omega,
+                            double domega, cudaStream_t st) {
+  BGK_FORM_DISPATCH(f,
+      (k_tan_step<F64><<<DIAG_BLOCKS, DIAG_THREADS, 0, st>>>(pops<const double>(f), pops<const double>(df),
+                                                             pops<double>(f2), pops<double>(df2), f.g, omega,
+                                                             domega)),
+      (k_tan_step<F32><<<DIAG_BLOCKS, DIAG_THREADS, 0, st>>>(pops<const float>(f), pops<const float>(df),
+                                                             pops<float>(f2), pops<float>(df2), f.g, (float)omega,
+                                                             (float)domega)))
+}
+
+cudaError_t launch_tan_loss(const Lattice& f, const Lattice& df, const double* ut, double* acc, cudaStream_t st) {
+  BGK_FORM_DISPATCH(f,
+      (k_tan_loss<F64><<<DIAG_BLOCKS, DIAG_THREADS, 0, st>>>(pops<const double>(f), pops<const double>(df), f.g, ut,
+                                                             acc)),
+      (k_tan_loss<F32><<<DIAG_BLOCKS, DIAG_THREADS, 0, st>>>(pops<const float>(f), pops<const float>(df), f.g, ut,
+                                                             acc)))
+}
+
+cudaError_t launch_acc_total(const double* acc, double* total, cudaStream_t st) {
+  k_acc_total<<<1, DIAG_THREADS, 0, st>>>(acc, total);
+  return cudaGetLastError();
+}
+
+}  // namespace bgk

@@ -709,6 +709,191 @@ int bgk_spectrum(bgk_ctx* c, int nbins, double* ek) {
   return BGK_OK;
 }
 
+// ------------------------------------------------------------------ adjoint
+namespace {
+
+// Device buffers owned by one adjoint / tangent call.
+struct AdjBufs {
+  std::vector<void*> mem;
+  ~AdjBufs() {
+    for (void* p : mem) cudaFree(p);
+  }
+  int alloc(void** p, size_t bytes, const char* what) {
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+      (void)cudaGetLastError();
+      *p = nullptr;
+      set_err("cudaMalloc(%zu bytes) for %s: %s", bytes, what, cudaGetErrorString(e));
+      return e == cudaErrorMemoryAllocation ? BGK_ERR_NOMEM : BGK_ERR_CUDA;
+    }
+    mem.push_back(*p);
+    return BGK_OK;
+  }
+  int lattice(const bgk_ctx* c, Lattice* L, const char* what) {
+    void* m = nullptr;
+    int rc = alloc(&m, (size_t)Q * c->g.qs * c->es, what);
+    if (rc) return rc;
+    L->form = c->form;
+    L->g = c->g;
+    for (int q = 0; q < Q; ++q) L->p[q] = (char*)m + (size_t)q * c->g.qs * c->es;
+    return BGK_OK;
+  }
+};
+
+int adj_check(bgk_ctx* c, int nsteps) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (c->form == FORM_F16) {
+    set_err("the adjoint and tangent models support the FP64 and FP32 forms");
+    return BGK_ERR_INVALID;
+  }
+  if (nsteps < 1) {
+    set_err("nsteps must be >= 1");
+    return BGK_ERR_INVALID;
+  }
+  return BGK_OK;
+}
+
+int upload3(AdjBufs& B, bgk_ctx* c, const double* a, const double* b, const double* d, double** out,
+            const char* what) {
+  const size_t n = (size_t)ncell(c);
+  int rc = B.alloc((void**)out, 3 * n * sizeof(double), what);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(*out, a, n * 8, cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(*out + n, b, n * 8, cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(*out + 2 * n, d, n * 8, cudaMemcpyHostToDevice, c->st));
+  return BGK_OK;
+}
+
+}  // namespace
+
+int bgk_adjoint(bgk_ctx* c, const double* u0, const double* v0, const double* w0, const double* ut, const double* vt,
+                const double* wt, int nsteps, int ckpt_every, double* loss, double* grad_u0, double* grad_tau) {
+  int rc = adj_check(c, nsteps);
+  if (rc) return rc;
+  if (!u0 || !v0 || !w0 || !ut || !vt || !wt || !loss || ckpt_every < 1) {
+    set_err("bgk_adjoint: invalid argument");
+    return BGK_ERR_INVALID;
+  }
+  CK(cudaSetDevice(c->p.device));
+  const int T = nsteps, K = ckpt_every < nsteps ? ckpt_every : nsteps;
+  const int nck = (T + K - 1) / K;
+  const int nwork = K - 1 > 2 ? K - 1 : 2;
+  const bool want_grad = grad_u0 || grad_tau;
+  AdjBufs B;
+  double *du0 = nullptr, *dut = nullptr, *acc = nullptr, *tot = nullptr;
+  if ((rc = upload3(B, c, u0, v0, w0, &du0, "initial velocity"))) return rc;
+  if ((rc = upload3(B, c, ut, vt, wt, &dut, "target velocity"))) return rc;
+  if ((rc = B.alloc((void**)&acc, 2 * DIAG_BLOCKS * sizeof(double), "adjoint sums"))) return rc;
+  if ((rc = B.alloc((void**)&tot, 2 * sizeof(double), "adjoint totals"))) return rc;
+  std::vector<Lattice> ck(want_grad ? nck : 1), work(nwork), lam(2);
+  for (auto& L : ck)
+    if ((rc = B.lattice(c, &L, "checkpoint"))) return rc;
+  for (auto& L : work)
+    if ((rc = B.lattice(c, &L, "recomputed state"))) return rc;
+  for (auto& L : lam)
+    if ((rc = B.lattice(c, &L, "adjoint state"))) return rc;
+  // forward: f^0 = equilibrium of u0 at rho = 1, checkpoints every K steps
+  const size_t n = (size_t)ncell(c);
+  CK(launch_init_velocity(ck[0], LAY_TWO, du0, du0 + n, du0 + 2 * n, 1.0, 0, c->g.nz, 1.0, nullptr, c->st));
+  const Lattice* cur = &ck[0];
+  int wi = 0;
+  for (int t = 0; t < T; ++t) {
+    const Lattice* next;
+    if (want_grad && t + 1 < T && (t + 1) % K == 0) next = &ck[(t + 1) / K];
+    else {
+      if (cur == &work[wi]) wi ^= 1;
+      next = &work[wi];
+    }
+    CK(launch_step_out_of_place(*cur, *next, c->omega, c->st));
+    cur = next;
+  }
+  CK(cudaMemsetAsync(acc, 0, 2 * DIAG_BLOCKS * sizeof(double), c->st));
+  CK(launch_adj_terminal(*cur, dut, lam[0], acc, c->st));
+  CK(launch_acc_total(acc, tot, c->st));
+  c->launches += T + 3;
+  if (want_grad) {
+    // backward over the segments, recomputing each from its checkpoint
+    CK(cudaMemsetAsync(acc, 0, 2 * DIAG_BLOCKS * sizeof(double), c->st));
+    int li = 0;  // lam[li] holds lam^{t+1}
+    for (int s = nck - 1; s >= 0; --s) {
+      const int t0 = s * K, t1 = t0 + K < T ? t0 + K : T;
+      std::vector<const Lattice*> st(t1 - t0);
+      st[0] = &ck[s];
+      for (int m = 1; m < t1 - t0; ++m) {
+        CK(launch_step_out_of_place(*st[m - 1], work[m - 1], c->omega, c->st));
+        st[m] = &work[m - 1];
+      }
+      for (int t = t1 - 1; t >= t0; --t) {
+        CK(launch_adj_step(*st[t - t0], lam[li], lam[li ^ 1], c->omega, acc, c->st));
+        li ^= 1;
+      }
+      c->launches += 2 * (t1 - t0) - 1;
+    }
+    CK(launch_acc_total(acc, tot + 1, c->st));
+    if (grad_u0) {
+      double* dg = nullptr;
+      if ((rc = B.alloc((void**)&dg, 3 * n * sizeof(double), "gradient"))) return rc;
+      CK(launch_adj_grad_u0(lam[li], du0, dg, c->st));
+      CK(cudaMemcpyAsync(grad_u0, dg, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+      c->launches++;
+    }
+  }
+  double h[2] = {0.0, 0.0};
+  CK(cudaMemcpyAsync(h, tot, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  *loss = h[0] / (double)n;
+  if (grad_tau) *grad_tau = -c->omega * c->omega * h[1];  // tau = 1/omega
+  return BGK_OK;
+}
+
+int bgk_tangent(bgk_ctx* c, const double* u0, const double* v0, const double* w0, const double* du0,
+                const double* dv0, const double* dw0, double dtau, const double* ut, const double* vt, const double* wt,
+                int nsteps, double* loss, double* dloss) {
+  int rc = adj_check(c, nsteps);
+  if (rc) return rc;
+  if (!u0 || !v0 || !w0 || !du0 || !dv0 || !dw0 || !ut || !vt || !wt || !loss || !dloss) {
+    set_err("bgk_tangent: invalid argument");
+    return BGK_ERR_INVALID;
+  }
+  CK(cudaSetDevice(c->p.device));
+  AdjBufs B;
+  double *d_u0 = nullptr, *d_du = nullptr, *dut = nullptr, *acc = nullptr, *tot = nullptr;
+  if ((rc = upload3(B, c, u0, v0, w0, &d_u0, "initial velocity"))) return rc;
+  if ((rc = upload3(B, c, du0, dv0, dw0, &d_du, "velocity perturbation"))) return rc;
+  if ((rc = upload3(B, c, ut, vt, wt, &dut, "target velocity"))) return rc;
+  if ((rc = B.alloc((void**)&acc, 2 * DIAG_BLOCKS * sizeof(double), "tangent sums"))) return rc;
+  if ((rc = B.alloc((void**)&tot, 2 * sizeof(double), "tangent totals"))) return rc;
+  Lattice f[2], df[2], scratch;
+  for (int m = 0; m < 2; ++m) {
+    if ((rc = B.lattice(c, &f[m], "state"))) return rc;
+    if ((rc = B.lattice(c, &df[m], "tangent state"))) return rc;
+  }
+  if ((rc = B.lattice(c, &scratch, "scratch"))) return rc;
+  const size_t n = (size_t)ncell(c);
+  CK(launch_init_velocity(f[0], LAY_TWO, d_u0, d_u0 + n, d_u0 + 2 * n, 1.0, 0, c->g.nz, 1.0, nullptr, c->st));
+  CK(launch_tan_init(df[0], d_u0, d_du, c->st));
+  const double domega = -c->omega * c->omega * dtau;  // omega = 1/tau
+  int cur = 0;
+  for (int t = 0; t < nsteps; ++t) {
+    CK(launch_tan_step(f[cur], df[cur], f[cur ^ 1], df[cur ^ 1], c->omega, domega, c->st));
+    cur ^= 1;
+  }
+  CK(cudaMemsetAsync(acc, 0, 2 * DIAG_BLOCKS * sizeof(double), c->st));
+  CK(launch_adj_terminal(f[cur], dut, scratch, acc, c->st));
+  CK(launch_acc_total(acc, tot, c->st));
+  CK(cudaMemsetAsync(acc, 0, 2 * DIAG_BLOCKS * sizeof(double), c->st));
+  CK(launch_tan_loss(f[cur], df[cur], dut, acc, c->st));
+  CK(launch_acc_total(acc, tot + 1, c->st));
+  c->launches += nsteps + 6;
+  double h[2] = {0.0, 0.0};
+  CK(cudaMemcpyAsync(h, tot, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  *loss = h[0] / (double)n;
+  *dloss = h[1] / (double)n;
+  return BGK_OK;
+}
+
 int bgk_get_scale(const bgk_ctx* c, double* s) {
   if (!c || !s) return BGK_ERR_INVALID;
   *s = c->scale;

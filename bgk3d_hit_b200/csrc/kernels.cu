@@ -12,6 +12,7 @@
 //   k_enstrophy  0.5|curl u|^2 from the local velocity field
 //   k_shift3     shift-only stencil of SRC/do_somethingGPU.F90:37-100
 #include "kernels.h"
+#include "reduce.cuh"
 
 namespace bgk {
 
@@ -72,7 +73,9 @@ __global__ void __launch_bounds__(256) k_two(Pops<const typename F::S> src, Pops
     const int jj = cyq(q) > 0 ? jm : (cyq(q) < 0 ? jp : j);
     const int kk = czq(q) > 0 ? km : (czq(q) < 0 ? kp : k);
     const int off = ii + g.sx * (jj + g.ny * kk);
-    v[q] = (q == Q - 1) ? dst.p[Q - 1][off] : ldg(src.p[q] + off);
+    // pop 19 with a plain load: in the time loop it is updated in place
+    // (src.p[18] == dst.p[18]); the adjoint's out-of-place steps pass distinct arrays
+    v[q] = (q == Q - 1) ? src.p[Q - 1][off] : ldg(src.p[q] + off);
   }
   F::cell(v, K);
   const int o = i + g.sx * (j + g.ny * k);
@@ -443,33 +446,6 @@ __global__ void k_import(Pops<typename F::S> a, Geo g, int q, const typename F::
 }
 
 // ------------------------------------------------------------ diagnostics
-struct KS { double s, c; };
-// Neumaier step; explicit _rn operations keep it free of FMA contraction.
-__device__ __forceinline__ void kadd(KS& a, double v) {
-  const double t = __dadd_rn(a.s, v);
-  if (fabs(a.s) >= fabs(v)) a.c = __dadd_rn(a.c, __dadd_rn(__dsub_rn(a.s, t), v));
-  else a.c = __dadd_rn(a.c, __dadd_rn(__dsub_rn(v, t), a.s));
-  a.s = t;
-}
-__device__ __forceinline__ void kcomb(KS& a, const KS& b) {
-  kadd(a, b.s);
-  a.c = __dadd_rn(a.c, b.c);
-}
-
-// Fixed-order block reduction of one quantity; thread 0 returns the result.
-__device__ __forceinline__ KS block_reduce(KS v, KS* sh) {
-  const int t = threadIdx.x;
-  sh[t] = v;
-  __syncthreads();
-  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
-    if (t < s) { KS a = sh[t]; kcomb(a, sh[t + s]); sh[t] = a; }
-    __syncthreads();
-  }
-  KS r = sh[0];
-  __syncthreads();
-  return r;
-}
-
 // Quantities: 0 rho, 1 ux, 2 uy, 3 uz, 4 0.5|u|^2 (local populations,
 // SRC/diagno.F90:96-111); 5 0.5|u|^2, 6 2*svisc*Ptotal (pulled populations,
 // SRC/dissipation.F90:76-249); 7 2*nu*S:S with S = -3*omega*Pi/(2*rho);
@@ -687,6 +663,20 @@ static cudaError_t two_impl(const Lattice& s, const Lattice& d, const StepK& K, 
   Shape sh = cell_shape(s.g);
   k_two<F><<<sh.grid, sh.block, 0, st>>>(ps, pd, s.g, K);
   return cudaGetLastError();
+}
+
+cudaError_t launch_step_out_of_place(const Lattice& src, const Lattice& dst, double omega, cudaStream_t st) {
+  const StepK K = make_stepk(src.form, omega, 1.0);
+  const Shape sh = cell_shape(src.g);
+  switch (src.form) {
+    case FORM_F64:
+      k_two<F64><<<sh.grid, sh.block, 0, st>>>(pops_of<const double>(src), pops_of<double>(dst), src.g, K);
+      return cudaGetLastError();
+    case FORM_F32:
+      k_two<F32><<<sh.grid, sh.block, 0, st>>>(pops_of<const float>(src), pops_of<float>(dst), src.g, K);
+      return cudaGetLastError();
+  }
+  return cudaErrorInvalidValue;
 }
 
 cudaError_t launch_two_lattice(const Lattice& src, const Lattice& dst, double omega, double scale, int variant,

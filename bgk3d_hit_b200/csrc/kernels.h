@@ -38,6 +38,30 @@ StepK make_stepk(int form, double omega, double scale);
 // back to 1 where the box does not fit it).
 cudaError_t launch_two_lattice(const Lattice& src, const Lattice& dst, double omega, double scale, int variant,
                                cudaStream_t st);
+// One step src -> dst with all 19 populations written to dst (pop 19 too);
+// FP64 and FP32 forms (used by the adjoint's recomputation).
+cudaError_t launch_step_out_of_place(const Lattice& src, const Lattice& dst, double omega, cudaStream_t st);
+
+// ------------------------------------------------------------- adjoint
+// Terminal adjoint and loss: lam = dL/df for L = 0.5 mean|u(f) - u_tgt|^2;
+// the loss is accumulated into acc (one compensated pair per block).
+cudaError_t launch_adj_terminal(const Lattice& f, const double* ut, const Lattice& lam, double* acc, cudaStream_t st);
+// lam_out = (d step / d f_t)^T lam_in, with f_t the state before the step;
+// accumulates -sum(lam_in . (g - e)) = dL/domega of this step into acc.
+cudaError_t launch_adj_step(const Lattice& ft, const Lattice& lam_in, const Lattice& lam_out, double omega,
+                            double* acc, cudaStream_t st);
+// dL/du0 (3 dense arrays) from lam at t = 0 and the initial velocity u0.
+cudaError_t launch_adj_grad_u0(const Lattice& lam0, const double* u0, double* grad, cudaStream_t st);
+// Tangent-linear model: perturbation of the initial state from du0 ...
+cudaError_t launch_tan_init(const Lattice& df, const double* u0, const double* du0, cudaStream_t st);
+// ... one step of (f, df) -> (f', df') with omega perturbed by domega ...
+cudaError_t launch_tan_step(const Lattice& f, const Lattice& df, const Lattice& f2, const Lattice& df2, double omega,
+                            double domega, cudaStream_t st);
+// ... and dL = mean (u - u_tgt).du at the final state into acc.
+cudaError_t launch_tan_loss(const Lattice& f, const Lattice& df, const double* ut, double* acc, cudaStream_t st);
+// Sums the per-block pairs of acc (DIAG_BLOCKS pairs) into *total.
+cudaError_t launch_acc_total(const double* acc, double* total, cudaStream_t st);
+
 // AA pattern: even (local read, reversed local write) or odd (pull from
 // neighbours' opposite slots, push to neighbours). variant as above (1 or 8).
 cudaError_t launch_aa(const Lattice& a, int odd, double omega, double scale, int variant, cudaStream_t st);

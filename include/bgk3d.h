@@ -165,6 +165,29 @@ int bgk_get_velocity(bgk_ctx* ctx, double* u, double* v, double* w);
    k = 0..nbins-1 (cuFFT). No reference counterpart. */
 int bgk_spectrum(bgk_ctx* ctx, int nbins, double* ek);
 
+/* Discrete adjoint of the time loop (no reference counterpart). From the
+   initial velocity (u0, v0, w0) (equilibrium at rho = 1, as bgk_init_velocity),
+   runs nsteps stream-collide steps with the context's omega, and computes
+   loss = 0.5 mean |u(T) - u_tgt|^2 over the box (u: local velocity of the final
+   populations), grad_u0 = dloss/d(u0, v0, w0) (3 blocks of lx*ly*lz doubles)
+   and grad_tau = dloss/dtau, tau = 1/omega. The backward pass recomputes the
+   forward from checkpoints stored every ckpt_every steps (about sqrt(nsteps)
+   keeps memory at (nsteps/ckpt_every + ckpt_every + 2) lattices). grad_u0 and
+   grad_tau may be NULL (with both NULL only the loss is computed). FP64 and
+   FP32 forms; uses its own device buffers and leaves the context's
+   populations unchanged. Synchronous. */
+int bgk_adjoint(bgk_ctx* ctx, const double* u0, const double* v0, const double* w0, const double* u_tgt,
+                const double* v_tgt, const double* w_tgt, int nsteps, int ckpt_every, double* loss,
+                double* grad_u0, double* grad_tau);
+
+/* Tangent-linear run (forward-mode derivative) of the same loss: dloss is the
+   derivative of loss along the perturbation (du0, dv0, dw0) of the initial
+   velocity and dtau of tau. Used to check bgk_adjoint:
+   dloss == <grad_u0, du> + grad_tau * dtau. FP64 and FP32 forms. */
+int bgk_tangent(bgk_ctx* ctx, const double* u0, const double* v0, const double* w0, const double* du0,
+                const double* dv0, const double* dw0, double dtau, const double* u_tgt, const double* v_tgt,
+                const double* w_tgt, int nsteps, double* loss, double* dloss);
+
 /* Scale of the FP16 form (1.0 for the other forms). */
 int bgk_get_scale(const bgk_ctx* ctx, double* scale);
 /* omega in use (SRC/hencol.F90:31 in the form's arithmetic, or the override). */

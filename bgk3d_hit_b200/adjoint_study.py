@@ -12,7 +12,11 @@ Loss = 0.5 mean |u(T) - u_tgt|^2. Reports, as one JSON object:
 - tangent: the relative difference between <grad, d> + grad_tau dtau and the
   tangent-linear derivative along (d, dtau) for a few directions;
 - cost: wall time of the adjoint call (forward with checkpoints, recomputation,
-  backward) over the wall time of a forward-only call of the same length.
+  backward) over the wall time of a forward-only call of the same length;
+- vs_fp64 (FP32 storage only): the relative L2 difference between the FP32
+  gradient and the FP64 adjoint gradient of the same problem (central
+  differences of an FP32 loss over 1000 steps are dominated by its rounding,
+  so the FP32 gradient is judged against FP64 instead).
 """
 from __future__ import annotations
 
@@ -90,14 +94,23 @@ def run(size=128, steps=1000, ckpt=32, tau=0.51, k0=4.0, u_rms=0.03, dirs=64, h=
         pred = float(np.dot(g, d.reshape(-1))) + gtau * dtau
         tan_errs.append(abs(pred - dl.value) / abs(dl.value))
     box.close()
+    vs64 = None
+    if precision != "fp64":
+        b64 = BGK3D(size, svisc=svisc, u0=u_rms, precision="fp64")
+        _, g64, gt64 = _adj(b64, u0, ut, steps, ckpt, True)
+        b64.close()
+        vs64 = {"grad_rel_l2": float(np.linalg.norm(g - g64) / np.linalg.norm(g64)),
+                "grad_tau_rel": abs(gtau - gt64) / abs(gt64)}
     return {
         "config": {"size": size, "steps": steps, "ckpt_every": ckpt, "tau": tau_used, "k0": k0, "u_rms": u_rms,
                    "precision": precision, "h": h, "directions": dirs},
         "loss": loss, "loss_in_adjoint_call": loss2, "grad_tau": gtau, "fd_grad_tau": fd_tau,
         "fd": {"max_rel_err": float(np.max(errs)), "median_rel_err": float(np.median(errs)),
+               "p90_rel_err": float(np.percentile(errs, 90)),
                "tau_rel_err": abs(gtau - fd_tau) / abs(fd_tau)},
         "tangent": {"max_rel_err": float(np.max(tan_errs)), "directions": ntan},
         "cost": {"forward_s": t_fwd, "adjoint_s": t_adj, "adjoint_over_forward": t_adj / t_fwd},
+        "vs_fp64": vs64,
     }
 
 

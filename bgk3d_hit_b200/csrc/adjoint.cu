@@ -12,9 +12,10 @@
 //             de_p = w_p [(1 + P_p) drho + rho (3 (c_p.du)(1 + 3 c_p.u) - 3 u.du)],
 //             drho = sum dg, du = (dj - u drho)/rho.
 // The initial state f0_q = w_q P_q(u0) (rho = 1, the equilibrium of
-// bgk_init_velocity) gives dL/du0 = B(lam_0, u0). The forward arithmetic of
-// the step (rho, u, e) is the library's own (equilibrium<V>), so the adjoint
-// differentiates exactly the map that bgk_col_mc applies.
+// bgk_init_velocity) gives dL/du0 = B(lam_0, u0). The adjoint step evaluates
+// rho, u and e of the forward state with fused multiply-adds; the tangent
+// model uses the forward's own arithmetic (equilibrium<V>), so the two agree
+// to the rounding of these terms.
 //
 // Kernels run a fixed grid (DIAG_BLOCKS x DIAG_THREADS) striding over the
 // cells, and accumulate their sums into one compensated pair per block, so
@@ -79,57 +80,87 @@ __global__ void __launch_bounds__(DIAG_THREADS) k_adj_terminal(Pops<const typena
   acc_block(loss, sh, acc);
 }
 
+// One cell per thread on the forward kernels' launch shape. The adjoint
+// arithmetic runs in the form's arithmetic type R (fused multiply-adds
+// allowed; e_p = w_p (rho (1 + P_p) - 1) from the P_p terms the adjoint needs
+// anyway), the dL/domega terms lam_p (e_p - g_p) are summed in double. lam is
+// read twice (the second time from cache) so that few values stay live. Each
+// block adds its dL/domega contribution (warp shuffles, then the eight warp
+// sums in order) into its own compensated pair acc[2*block].
 template <class F>
-__global__ void __launch_bounds__(DIAG_THREADS) k_adj_step(Pops<const typename F::S> ft, Pops<const typename F::S> lin,
-                                                           Pops<typename F::S> lout, Geo g, typename F::R omega,
-                                                           double* acc) {
-  using S = typename F::S; using R = typename F::R; using V = typename F::V; using N = Num<V>;
-  __shared__ KS sh[DIAG_THREADS];
-  KS dom = {0.0, 0.0};
-  const long long n = (long long)g.nx * g.ny * g.nz;
-  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
-    const int i = (int)(c % g.nx), j = (int)((c / g.nx) % g.ny), k = (int)(c / ((long long)g.nx * g.ny));
-    const long long o = i + (long long)g.sx * (j + (long long)g.ny * k);
-    long long off[Q];
-    V x[Q];
+__global__ void __launch_bounds__(256, sizeof(typename F::S) == 4 ? 4 : 2) k_adj_step(Pops<const typename F::S> ft, Pops<const typename F::S> lin,
+                                                  Pops<typename F::S> lout, Geo g, typename F::R omega, double* acc) {
+  using S = typename F::S; using R = typename F::R;
+  __shared__ double wsum[8];
+  double dw = 0.0;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  if (i < g.nx && j < g.ny) {
+    const int im = i == 0 ? g.nx - 1 : i - 1, ip = i == g.nx - 1 ? 0 : i + 1;
+    const int jm = j == 0 ? g.ny - 1 : j - 1, jp = j == g.ny - 1 ? 0 : j + 1;
+    const int km = k == 0 ? g.nz - 1 : k - 1, kp = k == g.nz - 1 ? 0 : k + 1;
+    const int o = i + g.sx * (j + g.ny * k);
+    auto offq = [&](int q) {
+      const int ii = cxq(q) > 0 ? im : (cxq(q) < 0 ? ip : i);
+      const int jj = cyq(q) > 0 ? jm : (cyq(q) < 0 ? jp : j);
+      const int kk = czq(q) > 0 ? km : (czq(q) < 0 ? kp : k);
+      return ii + g.sx * (jj + g.ny * kk);
+    };
+    R x[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) x[q] = (R)__ldg(ft.p[q] + offq(q));
+    R rho = (R)1, jx = 0, jy = 0, jz = 0;
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
-      const int ii = wrapa(i - cxq(q), g.nx), jj = wrapa(j - cyq(q), g.ny), kk = wrapa(k - czq(q), g.nz);
-      off[q] = ii + (long long)g.sx * (jj + (long long)g.ny * kk);
-      x[q] = V{ft.p[q][off[q]]};
+      rho += x[q];
+      jx += (R)cxq(q) * x[q];
+      jy += (R)cyq(q) * x[q];
+      jz += (R)czq(q) * x[q];
     }
-    V e[Q], vx, vy, vz;
-    (void)equilibrium<V>(x, e, vx, vy, vz);
-    const R ux = N::raw(vx), uy = N::raw(vy), uz = N::raw(vz);
-    const R usq = ux * ux + uy * uy + uz * uz;
+    const R ri = (R)1 / rho, ux = jx * ri, uy = jy * ri, uz = jz * ri;
+    const R a15 = (R)-1.5 * (ux * ux + uy * uy + uz * uz);
     R A = 0, L0 = 0, Lx = 0, Ly = 0, Lz = 0;
-    double dw = 0.0;
-    R lam[Q];
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
-      lam[q] = (R)lin.p[q][o];
+      const R lam = (R)__ldg(lin.p[q] + o);
       const R cu = cdot<R>(q, ux, uy, uz);
-      const R P = (R)3 * cu + (R)4.5 * cu * cu - (R)1.5 * usq;
-      const R wl = wq<R>(q) * lam[q];
+      const R P = cu * ((R)3 + (R)4.5 * cu) + a15;
+      const R w = wq<R>(q);
+      const R wl = w * lam;
       A += wl * ((R)1 + P);
       L0 += wl;
       const R t = wl * ((R)1 + (R)3 * cu);
       Lx += t * (R)cxq(q);
       Ly += t * (R)cyq(q);
       Lz += t * (R)czq(q);
-      dw -= (double)lam[q] * ((double)N::raw(x[q]) - (double)N::raw(e[q]));
+      const R e = w * (rho * ((R)1 + P) - (R)1);
+      dw += (double)lam * ((double)e - (double)x[q]);
     }
-    kadd(dom, dw);
-    const R Bx = (R)3 * Lx - (R)3 * ux * L0, By = (R)3 * Ly - (R)3 * uy * L0, Bz = (R)3 * Lz - (R)3 * uz * L0;
+    const R Bx = (R)3 * (Lx - ux * L0), By = (R)3 * (Ly - uy * L0), Bz = (R)3 * (Lz - uz * L0);
     const R G = A - (Bx * ux + By * uy + Bz * uz);
     const R om1 = (R)1 - omega;
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
-      const R mu = om1 * lam[q] + omega * (G + cdot<R>(q, Bx, By, Bz));
-      lout.p[q][off[q]] = (S)mu;  // reverse streaming: lam_t,q(x - c_q) = mu_q(x)
+      const R lam = (R)__ldg(lin.p[q] + o);
+      const R mu = om1 * lam + omega * (G + cdot<R>(q, Bx, By, Bz));
+      lout.p[q][offq(q)] = (S)mu;  // reverse streaming: lam_t,q(x - c_q) = mu_q(x)
     }
   }
-  acc_block(dom, sh, acc);
+  // fixed-order block sum into this block's running pair
+  for (int sft = 16; sft > 0; sft >>= 1) dw += __shfl_down_sync(0xffffffffu, dw, sft);
+  const int t = threadIdx.x + blockDim.x * threadIdx.y;
+  if ((t & 31) == 0) wsum[t >> 5] = dw;
+  __syncthreads();
+  if (t == 0) {
+    double s = 0.0;
+    for (int w = 0; w < 8; ++w) s += wsum[w];
+    const long long b = blockIdx.x + (long long)gridDim.x * (blockIdx.y + (long long)gridDim.y * blockIdx.z);
+    KS a2{acc[2 * b], acc[2 * b + 1]};
+    kadd(a2, s);
+    acc[2 * b] = a2.s;
+    acc[2 * b + 1] = a2.c;
+  }
 }
 
 template <class F>
@@ -260,6 +291,24 @@ __global__ void __launch_bounds__(DIAG_THREADS) k_acc_total(const double* __rest
   if (threadIdx.x == 0) *total = __dadd_rn(r.s, r.c);
 }
 
+// Launch shape of the per-cell kernels (x rows in blockDim.x, 256 threads).
+void adj_shape(const Geo& g, dim3* grid, dim3* block) {
+  const int tx = g.nx >= 128 ? 128 : ((g.nx + 31) / 32) * 32;
+  const int ty = 256 / tx;
+  *block = dim3(tx, ty, 1);
+  *grid = dim3((g.nx + tx - 1) / tx, (g.ny + ty - 1) / ty, g.nz);
+}
+
+// Sums n compensated pairs in a fixed order into *total.
+__global__ void __launch_bounds__(DIAG_THREADS) k_acc_total_n(const double* __restrict__ acc, long long n,
+                                                              double* total) {
+  __shared__ KS sh[DIAG_THREADS];
+  KS a = {0.0, 0.0};
+  for (long long b = threadIdx.x; b < n; b += blockDim.x) kcomb(a, KS{acc[2 * b], acc[2 * b + 1]});
+  const KS r = block_reduce(a, sh);
+  if (threadIdx.x == 0) *total = __dadd_rn(r.s, r.c);
+}
+
 template <class S> Pops<S> pops(const Lattice& L) {
   Pops<S> p;
   for (int q = 0; q < Q; ++q) p.p[q] = (S*)L.p[q];
@@ -281,13 +330,26 @@ cudaError_t launch_adj_terminal(const Lattice& f, const double* ut, const Lattic
       (k_adj_terminal<F32><<<DIAG_BLOCKS, DIAG_THREADS, 0, st>>>(pops<const float>(f), f.g, ut, pops<float>(lam), acc)))
 }
 
+long long adj_step_blocks(const Geo& g) {
+  dim3 grid, block;
+  adj_shape(g, &grid, &block);
+  return (long long)grid.x * grid.y * grid.z;
+}
+
 cudaError_t launch_adj_step(const Lattice& ft, const Lattice& lin, const Lattice& lout, double omega, double* acc,
                             cudaStream_t st) {
+  dim3 grid, block;
+  adj_shape(ft.g, &grid, &block);
   BGK_FORM_DISPATCH(ft,
-      (k_adj_step<F64><<<DIAG_BLOCKS, DIAG_THREADS, 0, st>>>(pops<const double>(ft), pops<const double>(lin),
-                                                             pops<double>(lout), ft.g, omega, acc)),
-      (k_adj_step<F32><<<DIAG_BLOCKS, DIAG_THREADS, 0, st>>>(pops<const float>(ft), pops<const float>(lin),
-                                                             pops<float>(lout), ft.g, (float)omega, acc)))
+      (k_adj_step<F64><<<grid, block, 0, st>>>(pops<const double>(ft), pops<const double>(lin), pops<double>(lout),
+                                               ft.g, omega, acc)),
+      (k_adj_step<F32><<<grid, block, 0, st>>>(pops<const float>(ft), pops<const float>(lin), pops<float>(lout),
+                                               ft.g, (float)omega, acc)))
+}
+
+cudaError_t launch_acc_total_n(const double* acc, long long n, double* total, cudaStream_t st) {
+  k_acc_total_n<<<1, DIAG_THREADS, 0, st>>>(acc, n, total);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_adj_grad_u0(const Lattice& lam0, const double* u0, double* grad, cudaStream_t st) {

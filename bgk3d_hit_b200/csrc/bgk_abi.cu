@@ -75,6 +75,12 @@ struct bgk_ctx {
   int plan_ok = 0;
   double* d_bins = nullptr;
   int nbins_alloc = 0;
+  // adjoint / tangent buffers, kept for later calls (freed by bgk_destroy)
+  std::vector<void*> lat_pool;   // lattice-sized blocks (Q * qs * es bytes)
+  double* vel_pool[4] = {nullptr, nullptr, nullptr, nullptr};  // 3*N doubles each
+  double* adj_acc = nullptr;
+  long long adj_acc_n = 0;
+  double* adj_tot = nullptr;
 };
 
 namespace {
@@ -405,6 +411,10 @@ int bgk_destroy(bgk_ctx* c) {
   cudaFree(c->stage);
   cudaFree(c->fft_buf);
   cudaFree(c->d_bins);
+  for (void* m : c->lat_pool) cudaFree(m);
+  for (double* m : c->vel_pool) cudaFree(m);
+  cudaFree(c->adj_acc);
+  cudaFree(c->adj_tot);
   if (c->h_tot) cudaFreeHost(c->h_tot);
   if (c->st) cudaStreamDestroy(c->st);
   delete c;
@@ -712,30 +722,43 @@ int bgk_spectrum(bgk_ctx* c, int nbins, double* ek) {
 // ------------------------------------------------------------------ adjoint
 namespace {
 
-// Device buffers owned by one adjoint / tangent call.
+// Hands out lattice-sized device blocks from the context's pool, growing it
+// on demand; the blocks stay allocated for later adjoint / tangent calls.
 struct AdjBufs {
-  std::vector<void*> mem;
-  ~AdjBufs() {
-    for (void* p : mem) cudaFree(p);
-  }
-  int alloc(void** p, size_t bytes, const char* what) {
-    cudaError_t e = cudaMalloc(p, bytes);
-    if (e != cudaSuccess) {
-      (void)cudaGetLastError();
-      *p = nullptr;
-      set_err("cudaMalloc(%zu bytes) for %s: %s", bytes, what, cudaGetErrorString(e));
-      return e == cudaErrorMemoryAllocation ? BGK_ERR_NOMEM : BGK_ERR_CUDA;
+  bgk_ctx* c;
+  size_t next = 0;
+  explicit AdjBufs(bgk_ctx* ctx) : c(ctx) {}
+  int lattice(Lattice* L, const char* what) {
+    if (next == c->lat_pool.size()) {
+      void* m = nullptr;
+      int rc = dev_alloc(c, &m, (size_t)Q * c->g.qs * c->es, what);
+      if (rc) return rc;
+      c->lat_pool.push_back(m);
     }
-    mem.push_back(*p);
-    return BGK_OK;
-  }
-  int lattice(const bgk_ctx* c, Lattice* L, const char* what) {
-    void* m = nullptr;
-    int rc = alloc(&m, (size_t)Q * c->g.qs * c->es, what);
-    if (rc) return rc;
+    void* m = c->lat_pool[next++];
     L->form = c->form;
     L->g = c->g;
     for (int q = 0; q < Q; ++q) L->p[q] = (char*)m + (size_t)q * c->g.qs * c->es;
+    return BGK_OK;
+  }
+  int sums(long long n, double** acc, double** tot) {
+    if (c->adj_acc_n < n) {
+      if (c->adj_acc) {
+        cudaFree(c->adj_acc);
+        c->dev_bytes -= 2 * c->adj_acc_n * (long long)sizeof(double);
+        c->adj_acc = nullptr;
+        c->adj_acc_n = 0;
+      }
+      int rc = dev_alloc(c, (void**)&c->adj_acc, 2 * (size_t)n * sizeof(double), "adjoint sums");
+      if (rc) return rc;
+      c->adj_acc_n = n;
+    }
+    if (!c->adj_tot) {
+      int rc = dev_alloc(c, (void**)&c->adj_tot, 2 * sizeof(double), "adjoint totals");
+      if (rc) return rc;
+    }
+    *acc = c->adj_acc;
+    *tot = c->adj_tot;
     return BGK_OK;
   }
 };
@@ -754,11 +777,16 @@ int adj_check(bgk_ctx* c, int nsteps) {
   return BGK_OK;
 }
 
-int upload3(AdjBufs& B, bgk_ctx* c, const double* a, const double* b, const double* d, double** out,
+// Uploads three host arrays of N doubles into velocity buffer `slot`.
+int upload3(bgk_ctx* c, int slot, const double* a, const double* b, const double* d, double** out,
             const char* what) {
   const size_t n = (size_t)ncell(c);
-  int rc = B.alloc((void**)out, 3 * n * sizeof(double), what);
-  if (rc) return rc;
+  if (!c->vel_pool[slot]) {
+    int rc = dev_alloc(c, (void**)&c->vel_pool[slot], 3 * n * sizeof(double), what);
+    if (rc) return rc;
+  }
+  *out = c->vel_pool[slot];
+  if (!a) return BGK_OK;  // buffer only (the gradient)
   CK(cudaMemcpyAsync(*out, a, n * 8, cudaMemcpyHostToDevice, c->st));
   CK(cudaMemcpyAsync(*out + n, b, n * 8, cudaMemcpyHostToDevice, c->st));
   CK(cudaMemcpyAsync(*out + 2 * n, d, n * 8, cudaMemcpyHostToDevice, c->st));
@@ -780,19 +808,19 @@ int bgk_adjoint(bgk_ctx* c, const double* u0, const double* v0, const double* w0
   const int nck = (T + K - 1) / K;
   const int nwork = K - 1 > 2 ? K - 1 : 2;
   const bool want_grad = grad_u0 || grad_tau;
-  AdjBufs B;
+  AdjBufs B(c);
   double *du0 = nullptr, *dut = nullptr, *acc = nullptr, *tot = nullptr;
-  if ((rc = upload3(B, c, u0, v0, w0, &du0, "initial velocity"))) return rc;
-  if ((rc = upload3(B, c, ut, vt, wt, &dut, "target velocity"))) return rc;
-  if ((rc = B.alloc((void**)&acc, 2 * DIAG_BLOCKS * sizeof(double), "adjoint sums"))) return rc;
-  if ((rc = B.alloc((void**)&tot, 2 * sizeof(double), "adjoint totals"))) return rc;
-  std::vector<Lattice> ck(want_grad ? nck : 1), work(nwork), lam(2);
+  if ((rc = upload3(c, 0, u0, v0, w0, &du0, "initial velocity"))) return rc;
+  if ((rc = upload3(c, 1, ut, vt, wt, &dut, "target velocity"))) return rc;
+  const long long nacc = adj_step_blocks(c->g) > DIAG_BLOCKS ? adj_step_blocks(c->g) : DIAG_BLOCKS;
+  if ((rc = B.sums(nacc, &acc, &tot))) return rc;
+  std::vector<Lattice> ck(want_grad ? nck : 1), work(want_grad ? nwork : 2), lam(want_grad ? 2 : 1);
   for (auto& L : ck)
-    if ((rc = B.lattice(c, &L, "checkpoint"))) return rc;
+    if ((rc = B.lattice(&L, "checkpoint"))) return rc;
   for (auto& L : work)
-    if ((rc = B.lattice(c, &L, "recomputed state"))) return rc;
+    if ((rc = B.lattice(&L, "recomputed state"))) return rc;
   for (auto& L : lam)
-    if ((rc = B.lattice(c, &L, "adjoint state"))) return rc;
+    if ((rc = B.lattice(&L, "adjoint state"))) return rc;
   // forward: f^0 = equilibrium of u0 at rho = 1, checkpoints every K steps
   const size_t n = (size_t)ncell(c);
   CK(launch_init_velocity(ck[0], LAY_TWO, du0, du0 + n, du0 + 2 * n, 1.0, 0, c->g.nz, 1.0, nullptr, c->st));
@@ -814,7 +842,7 @@ int bgk_adjoint(bgk_ctx* c, const double* u0, const double* v0, const double* w0
   c->launches += T + 3;
   if (want_grad) {
     // backward over the segments, recomputing each from its checkpoint
-    CK(cudaMemsetAsync(acc, 0, 2 * DIAG_BLOCKS * sizeof(double), c->st));
+    CK(cudaMemsetAsync(acc, 0, 2 * nacc * sizeof(double), c->st));
     int li = 0;  // lam[li] holds lam^{t+1}
     for (int s = nck - 1; s >= 0; --s) {
       const int t0 = s * K, t1 = t0 + K < T ? t0 + K : T;
@@ -830,10 +858,10 @@ int bgk_adjoint(bgk_ctx* c, const double* u0, const double* v0, const double* w0
       }
       c->launches += 2 * (t1 - t0) - 1;
     }
-    CK(launch_acc_total(acc, tot + 1, c->st));
+    CK(launch_acc_total_n(acc, adj_step_blocks(c->g), tot + 1, c->st));
     if (grad_u0) {
       double* dg = nullptr;
-      if ((rc = B.alloc((void**)&dg, 3 * n * sizeof(double), "gradient"))) return rc;
+      if ((rc = upload3(c, 2, nullptr, nullptr, nullptr, &dg, "gradient"))) return rc;
       CK(launch_adj_grad_u0(lam[li], du0, dg, c->st));
       CK(cudaMemcpyAsync(grad_u0, dg, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, c->st));
       c->launches++;
@@ -857,19 +885,18 @@ int bgk_tangent(bgk_ctx* c, const double* u0, const double* v0, const double* w0
     return BGK_ERR_INVALID;
   }
   CK(cudaSetDevice(c->p.device));
-  AdjBufs B;
+  AdjBufs B(c);
   double *d_u0 = nullptr, *d_du = nullptr, *dut = nullptr, *acc = nullptr, *tot = nullptr;
-  if ((rc = upload3(B, c, u0, v0, w0, &d_u0, "initial velocity"))) return rc;
-  if ((rc = upload3(B, c, du0, dv0, dw0, &d_du, "velocity perturbation"))) return rc;
-  if ((rc = upload3(B, c, ut, vt, wt, &dut, "target velocity"))) return rc;
-  if ((rc = B.alloc((void**)&acc, 2 * DIAG_BLOCKS * sizeof(double), "tangent sums"))) return rc;
-  if ((rc = B.alloc((void**)&tot, 2 * sizeof(double), "tangent totals"))) return rc;
+  if ((rc = upload3(c, 0, u0, v0, w0, &d_u0, "initial velocity"))) return rc;
+  if ((rc = upload3(c, 3, du0, dv0, dw0, &d_du, "velocity perturbation"))) return rc;
+  if ((rc = upload3(c, 1, ut, vt, wt, &dut, "target velocity"))) return rc;
+  if ((rc = B.sums(DIAG_BLOCKS, &acc, &tot))) return rc;
   Lattice f[2], df[2], scratch;
   for (int m = 0; m < 2; ++m) {
-    if ((rc = B.lattice(c, &f[m], "state"))) return rc;
-    if ((rc = B.lattice(c, &df[m], "tangent state"))) return rc;
+    if ((rc = B.lattice(&f[m], "state"))) return rc;
+    if ((rc = B.lattice(&df[m], "tangent state"))) return rc;
   }
-  if ((rc = B.lattice(c, &scratch, "scratch"))) return rc;
+  if ((rc = B.lattice(&scratch, "scratch"))) return rc;
   const size_t n = (size_t)ncell(c);
   CK(launch_init_velocity(f[0], LAY_TWO, d_u0, d_u0 + n, d_u0 + 2 * n, 1.0, 0, c->g.nz, 1.0, nullptr, c->st));
   CK(launch_tan_init(df[0], d_u0, d_du, c->st));

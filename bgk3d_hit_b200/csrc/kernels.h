@@ -47,7 +47,10 @@ cudaError_t launch_step_out_of_place(const Lattice& src, const Lattice& dst, dou
 // the loss is accumulated into acc (one compensated pair per block).
 cudaError_t launch_adj_terminal(const Lattice& f, const double* ut, const Lattice& lam, double* acc, cudaStream_t st);
 // lam_out = (d step / d f_t)^T lam_in, with f_t the state before the step;
-// accumulates -sum(lam_in . (g - e)) = dL/domega of this step into acc.
+// accumulates -sum(lam_in . (g - e)) = dL/domega of this step into acc, one
+// compensated pair per block of the launch (adj_step_blocks pairs).
+long long adj_step_blocks(const Geo& g);
+cudaError_t launch_acc_total_n(const double* acc, long long n, double* total, cudaStream_t st);
 cudaError_t launch_adj_step(const Lattice& ft, const Lattice& lam_in, const Lattice& lam_out, double omega,
                             double* acc, cudaStream_t st);
 // dL/du0 (3 dense arrays) from lam at t = 0 and the initial velocity u0.

@@ -174,7 +174,8 @@ int bgk_spectrum(bgk_ctx* ctx, int nbins, double* ek);
    forward from checkpoints stored every ckpt_every steps (about sqrt(nsteps)
    keeps memory at (nsteps/ckpt_every + ckpt_every + 2) lattices). grad_u0 and
    grad_tau may be NULL (with both NULL only the loss is computed). FP64 and
-   FP32 forms; uses its own device buffers and leaves the context's
+   FP32 forms; works in device buffers of its own, which stay allocated in the
+   context for later calls (bgk_destroy frees them), and leaves the context's
    populations unchanged. Synchronous. */
 int bgk_adjoint(bgk_ctx* ctx, const double* u0, const double* v0, const double* w0, const double* u_tgt,
                 const double* v_tgt, const double* w_tgt, int nsteps, int ckpt_every, double* loss,

@@ -103,9 +103,10 @@ static double now_s(void) {
 
 /* Timed CPU baseline: `steps` iterations of the reference loop body
    (boundaries + col_MC, SRC/bgk3d_HIT.F90:131,140) in double precision on an
-   already-initialised lattice. Returns elapsed seconds. */
+   already-initialised lattice, in the row-vectorised form (bit-identical to
+   orc_step_f64). Returns elapsed seconds. */
 double orc_time_steps_f64(orc_lat_f64 *L, double svisc, int steps) {
     double t0 = now_s();
-    for (int s = 0; s < steps; ++s) orc_step_f64(L, svisc);
+    for (int s = 0; s < steps; ++s) orc_step_rows_f64(L, svisc);
     return now_s() - t0;
 }

@@ -397,6 +397,83 @@ void FN(orc_step)(LAT *L, double svisc) {
     FN(orc_col_mc)(L, svisc, 0);
 }
 
+#ifndef FAST16
+/* The same step written for a CPU: per row, 19 source-row pointers into the
+   ghosted arrays and a vectorisable loop over i (each lane performs exactly
+   the operations of FN(equilibrium) and the relaxation, so the result is
+   bit-identical to orc_step). Used as the timed CPU baseline. */
+void FN(orc_step_rows)(LAT *L, double svisc) {
+    FN(orc_boundaries)(L);
+    const REAL omega = (REAL)FN(orc_omega)(svisc);
+    const long l = L->l, m = L->m, n = L->n;
+    const REAL uno = (REAL)1, cte1 = (REAL)1, cte0 = uno - cte1;
+    const REAL rf = (REAL)3.0, qf = (REAL)1.5, tre = (REAL)3.0;
+    const REAL p0 = (REAL)(1.0 / 3.0), p1 = (REAL)(1.0 / 18.0), p2 = (REAL)(1.0 / (3.0 * 3.0 * (1.0 + 3.0)));
+#pragma omp parallel for collapse(2) schedule(static)
+    for (long k = 1; k <= n; ++k)
+        for (long j = 1; j <= m; ++j) {
+            const STOR *restrict s[19];
+            STOR *restrict d[19];
+            for (int q = 0; q < 19; ++q) {
+                s[q] = L->a[q] + FN(gidx)(L, 1 - FN(CX)[q], j - FN(CY)[q], k - FN(CZ)[q]);
+                d[q] = (q < 18 ? L->b[q] : L->a[18]) + FN(gidx)(L, 1, j, k);
+            }
+#pragma omp simd
+            for (long i = 0; i < l; ++i) {
+                REAL x[19];
+                for (int q = 0; q < 19; ++q) x[q] = s[q][i];
+                REAL rho = x[0] + x[1] + x[2] + x[3] + x[4] + x[5] + x[6] + x[7]
+                         + x[8] + x[9] + x[10] + x[11] + x[12] + x[13] + x[14] + x[15]
+                         + x[16] + x[17] + x[18] + cte1;
+                REAL rhoinv = uno / rho;
+                REAL vx = (x[0] + x[1] + x[2] + x[3] + x[4] - x[9] - x[10] - x[11] - x[12] - x[13]) * rhoinv;
+                REAL vy = (x[2] + x[6] + x[7] + x[8] + x[11] - x[0] - x[9] - x[15] - x[16] - x[17]) * rhoinv;
+                REAL vz = (x[3] + x[5] + x[6] + x[12] + x[17] - x[1] - x[8] - x[10] - x[14] - x[15]) * rhoinv;
+                REAL vx2 = vx * vx, vy2 = vy * vy, vz2 = vz * vz;
+                REAL vsq = vx2 + vy2 + vz2;
+                REAL vxpy = vx + vy; REAL qxpy = cte0 + qf * (tre * vxpy * vxpy - vsq);
+                REAL vxmy = vx - vy; REAL qxmy = cte0 + qf * (tre * vxmy * vxmy - vsq);
+                REAL vxpz = vx + vz; REAL qxpz = cte0 + qf * (tre * vxpz * vxpz - vsq);
+                REAL vxmz = vx - vz; REAL qxmz = cte0 + qf * (tre * vxmz * vxmz - vsq);
+                REAL vypz = vy + vz; REAL qypz = cte0 + qf * (tre * vypz * vypz - vsq);
+                REAL vymz = vy - vz; REAL qymz = cte0 + qf * (tre * vymz * vymz - vsq);
+                REAL qx = cte0 + qf * (tre * vx2 - vsq);
+                REAL qy = cte0 + qf * (tre * vy2 - vsq);
+                REAL qz = cte0 + qf * (tre * vz2 - vsq);
+                REAL q0 = cte0 + qf * (-vsq);
+                vx = rf * vx; vy = rf * vy; vz = rf * vz;
+                vxpy = rf * vxpy; vxmy = rf * vxmy; vxpz = rf * vxpz;
+                vxmz = rf * vxmz; vypz = rf * vypz; vymz = rf * vymz;
+                REAL rp0 = rho * p0, rp1 = rho * p1, rp2 = rho * p2;
+                REAL e[19];
+                e[0]  = rp2 * (+vxmy + qxmy) + cte1 * (rp2 - p2);
+                e[1]  = rp2 * (+vxmz + qxmz) + cte1 * (rp2 - p2);
+                e[2]  = rp2 * (+vxpy + qxpy) + cte1 * (rp2 - p2);
+                e[3]  = rp2 * (+vxpz + qxpz) + cte1 * (rp2 - p2);
+                e[4]  = rp1 * (+vx + qx) + cte1 * (rp1 - p1);
+                e[5]  = rp1 * (+vz + qz) + cte1 * (rp1 - p1);
+                e[6]  = rp2 * (+vypz + qypz) + cte1 * (rp2 - p2);
+                e[7]  = rp1 * (+vy + qy) + cte1 * (rp1 - p1);
+                e[8]  = rp2 * (+vymz + qymz) + cte1 * (rp2 - p2);
+                e[9]  = rp2 * (-vxpy + qxpy) + cte1 * (rp2 - p2);
+                e[10] = rp2 * (-vxpz + qxpz) + cte1 * (rp2 - p2);
+                e[11] = rp2 * (-vxmy + qxmy) + cte1 * (rp2 - p2);
+                e[12] = rp2 * (-vxmz + qxmz) + cte1 * (rp2 - p2);
+                e[13] = rp1 * (-vx + qx) + cte1 * (rp1 - p1);
+                e[14] = rp1 * (-vz + qz) + cte1 * (rp1 - p1);
+                e[15] = rp2 * (-vypz + qypz) + cte1 * (rp2 - p2);
+                e[16] = rp1 * (-vy + qy) + cte1 * (rp1 - p1);
+                e[17] = rp2 * (-vymz + qymz) + cte1 * (rp2 - p2);
+                e[18] = rp0 * (+q0) + cte1 * (rp0 - p0);
+                for (int q = 0; q < 19; ++q) d[q][i] = ENC(L, x[q] - omega * (x[q] - e[q]));
+            }
+        }
+    for (int q = 0; q < 18; ++q) {
+        STOR *c = L->a[q]; L->a[q] = L->b[q]; L->b[q] = c;
+    }
+}
+#endif
+
 /* Neumaier-compensated accumulation in double. */
 typedef struct { double s, c; } FN(ksum);
 static inline void FN(kadd)(FN(ksum) *a, double v) {

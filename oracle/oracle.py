@@ -61,6 +61,8 @@ def lib():
             f("orc_col_mc_omega").argtypes = [vp, d, i]
             f("orc_col_mc").argtypes = [vp, d, i]
             f("orc_step").argtypes = [vp, d]
+            if suf != "_f16":
+                f("orc_step_rows").argtypes = [vp, d]
             f("orc_diagno").argtypes = [vp, i, dp]
             f("orc_dissipation").argtypes = [vp, d, d, i, i, dp]
             f("orc_extras").argtypes = [vp, d, dp]
@@ -145,6 +147,10 @@ class OracleLattice:
             self.col_mc(svisc, True)
         else:
             self._f("orc_step")(self.h, svisc)
+
+    def step_rows(self, svisc: float):
+        """boundaries + col_MC in the row-vectorised CPU form (bit-identical)."""
+        self._f("orc_step_rows")(self.h, svisc)
 
     def diagno(self, faithful: bool = False) -> np.ndarray:
         out = np.zeros(5)

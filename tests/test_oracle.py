@@ -43,6 +43,21 @@ def test_step3_ghost_fill_equals_modulo_indexing(oracle_mod, form, shape):
     assert np.array_equal(g.get_pops().view(np.uint8), p.get_pops().view(np.uint8))
 
 
+@pytest.mark.parametrize("form", ["f64", "f32"])
+def test_row_vectorised_step_is_bit_identical(oracle_mod, form):
+    """The timed CPU baseline (row pointers, vectorised i loop) gives the same
+    bits as the per-cell restatement."""
+    O = oracle_mod
+    a, b = O.OracleLattice(9, 7, 5, form=form), O.OracleLattice(9, 7, 5, form=form)
+    a.init_tgv(0.05, faithful=True)
+    b.put_pops(a.get_pops())
+    b.init_tgv(0.05, faithful=True)
+    for _ in range(6):
+        a.step(0.01)
+        b.step_rows(0.01)
+    assert np.array_equal(a.get_pops().view(np.uint8), b.get_pops().view(np.uint8))
+
+
 def test_edge_ghosts_hold_periodic_images(oracle_mod):
     """After boundaries, the 12 edge lines dumped by CORNER_CHECK
     (SRC/boundaries.F90:68-97) hold the periodic image of the interior."""

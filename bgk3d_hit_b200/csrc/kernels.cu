@@ -251,7 +251,8 @@ __global__ void __launch_bounds__(256, 4) k_two_f16v2(Pops<const __half> src, Po
 // Even step: g_q(x) = slot q at x; result q -> slot opp(q) at x.
 // Odd step:  g_q(x) = slot opp(q) at x - c_q; result q -> slot q at x + c_q.
 // Each thread reads exactly the locations it writes, so the update is
-// race-free in place.
+// race-free in place; a location is never read after it has been written,
+// which also makes the read-only load path safe.
 template <class F, bool ODD>
 __global__ void __launch_bounds__(256) k_aa(Pops<typename F::S> a, Geo g, StepK K) {
   using S = typename F::S;
@@ -260,33 +261,24 @@ __global__ void __launch_bounds__(256) k_aa(Pops<typename F::S> a, Geo g, StepK 
   const int k = blockIdx.z;
   if (i >= g.nx || j >= g.ny) return;
   const int o = i + g.sx * (j + g.ny * k);
+  const int im = i == 0 ? g.nx - 1 : i - 1, ip = i == g.nx - 1 ? 0 : i + 1;
+  const int jm = j == 0 ? g.ny - 1 : j - 1, jp = j == g.ny - 1 ? 0 : j + 1;
+  const int km = k == 0 ? g.nz - 1 : k - 1, kp = k == g.nz - 1 ? 0 : k + 1;
+  // location x - c_q (read, slot opp(q)) == location x + c_opp(q) (write, slot opp(q))
+  auto back = [&](int q) {
+    const int ii = cxq(q) > 0 ? im : (cxq(q) < 0 ? ip : i);
+    const int jj = cyq(q) > 0 ? jm : (cyq(q) < 0 ? jp : j);
+    const int kk = czq(q) > 0 ? km : (czq(q) < 0 ? kp : k);
+    return ii + g.sx * (jj + g.ny * kk);
+  };
   S v[Q];
-  int off[Q];
-  if (ODD) {
-    const int im = i == 0 ? g.nx - 1 : i - 1, ip = i == g.nx - 1 ? 0 : i + 1;
-    const int jm = j == 0 ? g.ny - 1 : j - 1, jp = j == g.ny - 1 ? 0 : j + 1;
-    const int km = k == 0 ? g.nz - 1 : k - 1, kp = k == g.nz - 1 ? 0 : k + 1;
 #pragma unroll
-    for (int q = 0; q < Q; ++q) {
-      // location x - c_q (read, slot opp(q)) == location x + c_opp(q) (write, slot opp(q))
-      const int ii = cxq(q) > 0 ? im : (cxq(q) < 0 ? ip : i);
-      const int jj = cyq(q) > 0 ? jm : (cyq(q) < 0 ? jp : j);
-      const int kk = czq(q) > 0 ? km : (czq(q) < 0 ? kp : k);
-      off[q] = ii + g.sx * (jj + g.ny * kk);
-    }
-#pragma unroll
-    for (int q = 0; q < Q; ++q) v[q] = a.p[oppq(q)][off[q]];
-  } else {
-#pragma unroll
-    for (int q = 0; q < Q; ++q) v[q] = a.p[q][o];
-  }
+  for (int q = 0; q < Q; ++q) v[q] = ODD ? ldg(a.p[oppq(q)] + back(q)) : ldg(a.p[q] + o);
   F::cell(v, K);
-  if (ODD) {
 #pragma unroll
-    for (int q = 0; q < Q; ++q) a.p[q][off[oppq(q)]] = v[q];
-  } else {
-#pragma unroll
-    for (int q = 0; q < Q; ++q) a.p[oppq(q)][o] = v[q];
+  for (int q = 0; q < Q; ++q) {
+    if (ODD) a.p[q][back(oppq(q))] = v[q];
+    else a.p[oppq(q)][o] = v[q];
   }
 }
 

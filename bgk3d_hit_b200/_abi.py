@@ -72,6 +72,9 @@ PROTOTYPES = [
     ("bgk_get_deviations", _i, [_vp, _dp]),
     ("bgk_get_velocity", _i, [_vp, _dp, _dp, _dp]),
     ("bgk_spectrum", _i, [_vp, _i, _dp]),
+    ("bgk_save", _i, [_vp, C.c_char_p]),
+    ("bgk_load", _i, [_vp, C.c_char_p]),
+    ("bgk_vtk", _i, [_vp, _i, _i, _i, C.c_char_p]),
     ("bgk_adjoint", _i, [_vp, _dp, _dp, _dp, _dp, _dp, _dp, _i, _i, _dp, _dp, _dp]),
     ("bgk_tangent", _i, [_vp, _dp, _dp, _dp, _dp, _dp, _dp, _d, _dp, _dp, _dp, _i, _dp, _dp]),
     ("bgk_get_scale", _i, [_vp, _dp]),

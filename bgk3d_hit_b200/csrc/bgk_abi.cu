@@ -5,8 +5,10 @@
 
 #include <cmath>
 #include <cstdarg>
+#include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <string>
 #include <vector>
 
 #include "bgk3d.h"
@@ -716,6 +718,165 @@ int bgk_spectrum(bgk_ctx* c, int nbins, double* ek) {
   }
   CK(cudaMemcpyAsync(ek, c->d_bins, (size_t)nbins * 8, cudaMemcpyDeviceToHost, c->st));
   CK(cudaStreamSynchronize(c->st));
+  return BGK_OK;
+}
+
+// --------------------------------------------------------------- file output
+namespace {
+
+constexpr char CKPT_MAGIC[8] = {'B', 'G', 'K', '3', 'D', 'C', 'K', '1'};
+
+struct CkptHeader {
+  char magic[8];
+  int32_t lx, ly, lz, precision;
+  int64_t step;
+  double scale, omega;
+};
+
+struct FileCloser {
+  FILE* f;
+  ~FileCloser() {
+    if (f) fclose(f);
+  }
+};
+
+}  // namespace
+
+int bgk_save(bgk_ctx* c, const char* path) {
+  int rc = check_init(c);
+  if (rc) return rc;
+  if (!path) {
+    set_err("bgk_save: null path");
+    return BGK_ERR_INVALID;
+  }
+  CK(cudaSetDevice(c->p.device));
+  FileCloser fc{fopen(path, "wb")};
+  if (!fc.f) {
+    set_err("bgk_save: cannot open %s for writing", path);
+    return BGK_ERR_INVALID;
+  }
+  CkptHeader h{};
+  std::memcpy(h.magic, CKPT_MAGIC, 8);
+  h.lx = c->g.nx; h.ly = c->g.ny; h.lz = c->g.nz; h.precision = c->form;
+  h.step = c->step; h.scale = c->scale; h.omega = c->omega;
+  if (fwrite(&h, sizeof(h), 1, fc.f) != 1) {
+    set_err("bgk_save: write failed on %s", path);
+    return BGK_ERR_INVALID;
+  }
+  const size_t n = (size_t)ncell(c);
+  rc = ensure_stage(c, n * 8);
+  if (rc) return rc;
+  std::vector<char> host(n * c->es);
+  for (int q = 0; q < Q; ++q) {
+    CK(launch_export(c->A, c->lay, q, c->stage, nullptr, c->scale, c->st));
+    c->launches++;
+    CK(cudaMemcpyAsync(host.data(), c->stage, n * c->es, cudaMemcpyDeviceToHost, c->st));
+    rc = sync_and_check(c);
+    if (rc) return rc;
+    if (fwrite(host.data(), c->es, n, fc.f) != n) {
+      set_err("bgk_save: write failed on %s", path);
+      return BGK_ERR_INVALID;
+    }
+  }
+  return BGK_OK;
+}
+
+int bgk_load(bgk_ctx* c, const char* path) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!path) {
+    set_err("bgk_load: null path");
+    return BGK_ERR_INVALID;
+  }
+  CK(cudaSetDevice(c->p.device));
+  FileCloser fc{fopen(path, "rb")};
+  if (!fc.f) {
+    set_err("bgk_load: cannot open %s", path);
+    return BGK_ERR_INVALID;
+  }
+  CkptHeader h{};
+  if (fread(&h, sizeof(h), 1, fc.f) != 1 || std::memcmp(h.magic, CKPT_MAGIC, 8) != 0) {
+    set_err("bgk_load: %s is not a checkpoint of this library", path);
+    return BGK_ERR_INVALID;
+  }
+  if (h.lx != c->g.nx || h.ly != c->g.ny || h.lz != c->g.nz || h.precision != c->form) {
+    set_err("bgk_load: %s holds a %dx%dx%d box in precision %d, the context is %dx%dx%d in precision %d", path, h.lx,
+            h.ly, h.lz, h.precision, c->g.nx, c->g.ny, c->g.nz, c->form);
+    return BGK_ERR_INVALID;
+  }
+  const size_t n = (size_t)ncell(c);
+  rc = ensure_stage(c, n * 8);
+  if (rc) return rc;
+  std::vector<char> host(n * c->es);
+  const int lay = init_layout(c);
+  for (int q = 0; q < Q; ++q) {
+    if (fread(host.data(), c->es, n, fc.f) != n) {
+      set_err("bgk_load: %s is truncated", path);
+      return BGK_ERR_INVALID;
+    }
+    CK(cudaMemcpyAsync(c->stage, host.data(), n * c->es, cudaMemcpyHostToDevice, c->st));
+    CK(launch_import(c->A, lay, q, c->stage, c->st));
+    c->launches++;
+    CK(cudaStreamSynchronize(c->st));
+  }
+  CK(cudaMemsetAsync(c->d_err, 0, sizeof(int), c->st));
+  CK(cudaStreamSynchronize(c->st));
+  c->lay = lay;
+  c->step = h.step;
+  if (c->form == FORM_F16) c->scale = h.scale;
+  c->initialized = 1;
+  return BGK_OK;
+}
+
+int bgk_vtk(bgk_ctx* c, int itime, int kind, int index, const char* dir) {
+  int rc = check_init(c);
+  if (rc) return rc;
+  const int nx = c->g.nx, ny = c->g.ny, nz = c->g.nz;
+  const int lim = kind == 1 ? nz : kind == 2 ? ny : kind == 3 ? nx : 1;
+  if (kind < 0 || kind > 3 || (kind > 0 && (index < 1 || index > lim)) || itime < 0 || itime > 99999999) {
+    set_err("bgk_vtk: invalid kind %d / index %d / itime %d", kind, index, itime);
+    return BGK_ERR_INVALID;
+  }
+  CK(cudaSetDevice(c->p.device));
+  const long long npts = kind == 1 ? (long long)nx * ny : kind == 2 ? (long long)nx * nz
+                       : kind == 3 ? (long long)ny * nz : ncell(c);
+  rc = ensure_stage(c, (size_t)npts * 12 > (size_t)ncell(c) * 8 ? (size_t)npts * 12 : (size_t)ncell(c) * 8);
+  if (rc) return rc;
+  CK(launch_vtk(c->A, c->lay, kind, index - 1, (float*)c->stage, npts, c->scale, c->st));
+  c->launches++;
+  std::vector<float> v((size_t)npts * 3);
+  CK(cudaMemcpyAsync(v.data(), c->stage, (size_t)npts * 12, cudaMemcpyDeviceToHost, c->st));
+  rc = sync_and_check(c);
+  if (rc) return rc;
+  // legacy VTK, as SRC/vtk_xy.binary.F90:58-97 writes it: ASCII header with
+  // I10 fields, then big-endian float32 velocity triples
+  static const char* tag[4] = {"3d", "xy", "xz", "yz"};
+  char name[64];
+  snprintf(name, sizeof(name), "tec_%s.%05d.%08d.vtk", tag[kind], 0, itime);
+  const std::string path = std::string(dir && *dir ? dir : ".") + "/" + name;
+  FileCloser fc{fopen(path.c_str(), "wb")};
+  if (!fc.f) {
+    set_err("bgk_vtk: cannot open %s", path.c_str());
+    return BGK_ERR_INVALID;
+  }
+  const int dims[4][3] = {{nx, ny, nz}, {nx, ny, 1}, {nx, 1, nz}, {1, ny, nz}};
+  const int orig[4][3] = {{1, 1, 1}, {1, 1, index}, {1, index, 1}, {index, 1, 1}};
+  fprintf(fc.f, "# vtk DataFile Version 2.0\nCampo\nBINARY\nDATASET STRUCTURED_POINTS\n");
+  fprintf(fc.f, "DIMENSIONS %10d %10d %10d\n", dims[kind][0], dims[kind][1], dims[kind][2]);
+  fprintf(fc.f, "ORIGIN %10d %10d %10d\n", orig[kind][0], orig[kind][1], orig[kind][2]);
+  fprintf(fc.f, "SPACING %10d %10d %10d\n", 1, 1, 1);
+  fprintf(fc.f, "POINT_DATA%10lld\n", npts);
+  fprintf(fc.f, "VECTORS velocity float \n");
+  std::vector<uint32_t> be(v.size());
+  for (size_t s = 0; s < v.size(); ++s) {
+    uint32_t b;
+    std::memcpy(&b, &v[s], 4);
+    be[s] = __builtin_bswap32(b);
+  }
+  if (fwrite(be.data(), 4, be.size(), fc.f) != be.size()) {
+    set_err("bgk_vtk: write failed on %s", path.c_str());
+    return BGK_ERR_INVALID;
+  }
   return BGK_OK;
 }
 

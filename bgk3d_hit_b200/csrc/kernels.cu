@@ -550,6 +550,37 @@ __global__ void k_last_zj(Pops<const typename F::S> a, Geo g, typename F::R inv,
   *out = (double)N::raw(uz);
 }
 
+// -------------------------------------------------------------------- VTK
+// Velocity j/rho of the points of a VTK slice or box, as float triples in the
+// file order of SRC/vtk_xy.binary.F90:79-97 (xy: j outer, i inner), vtk_xz
+// (k, i), vtk_yz (k, j) and vtk_3d (k, j, i). The sums are taken in the
+// storage arithmetic in the reference's order, each rounded to single
+// precision, then divided in single precision (u/den).
+template <class F, int LAY>
+__global__ void k_vtk(Pops<const typename F::S> a, Geo g, int kind, int index, float* out, long long npts,
+                      typename F::R inv) {
+  using V = typename F::V; using N = Num<V>;
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < npts; c += (long long)gridDim.x * blockDim.x) {
+    int i, j, k;
+    if (kind == 1) { i = (int)(c % g.nx); j = (int)(c / g.nx); k = index; }
+    else if (kind == 2) { i = (int)(c % g.nx); k = (int)(c / g.nx); j = index; }
+    else if (kind == 3) { j = (int)(c % g.ny); k = (int)(c / g.ny); i = index; }
+    else { i = (int)(c % g.nx); j = (int)((c / g.nx) % g.ny); k = (int)(c / ((long long)g.nx * g.ny)); }
+    V x[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) x[q] = N::wrap(F::dec(a.p[ref_slot<LAY>(q)][ref_off<LAY>(g, q, i, j, k, 0, 0, 0)], inv));
+    const V u = x[0] + x[1] + x[2] + x[3] + x[4] - x[9] - x[10] - x[11] - x[12] - x[13];
+    const V w = x[2] + x[6] + x[7] + x[8] + x[11] - x[0] - x[9] - x[15] - x[16] - x[17];
+    const V v = x[3] + x[5] + x[6] + x[12] + x[17] - x[1] - x[8] - x[10] - x[14] - x[15];
+    const V den = x[0] + x[1] + x[2] + x[3] + x[4] + x[5] + x[6] + x[7] + x[8] + x[9] + x[10] + x[11] + x[12] +
+                  x[13] + x[14] + x[15] + x[16] + x[17] + x[18] + N::c(1.0);
+    const float d = (float)N::raw(den);
+    out[3 * c + 0] = __fdiv_rn((float)N::raw(u), d);
+    out[3 * c + 1] = __fdiv_rn((float)N::raw(w), d);
+    out[3 * c + 2] = __fdiv_rn((float)N::raw(v), d);
+  }
+}
+
 // --------------------------------------------------------------- spectrum
 template <class C>
 __global__ void k_spec_bins(const C* __restrict__ f, int nx, int ny, int nz, int nbins, double* bins, double norm) {
@@ -863,6 +894,31 @@ cudaError_t launch_shift3(const void* const in[3], void* const out[3], int nx, i
   else
     return cudaErrorInvalidValue;
   return cudaGetLastError();
+}
+
+template <class F, int LAY>
+static void vtk_lay(const Lattice& a, int kind, int index, float* out, long long npts, double scale,
+                    cudaStream_t st) {
+  using S = typename F::S; using R = typename F::R;
+  k_vtk<F, LAY><<<grid_1d(npts, 256, 148 * 16), 256, 0, st>>>(pops_of<const S>(a), a.g, kind, index, out, npts,
+                                                               (R)(1.0 / scale));
+}
+template <class F>
+static cudaError_t vtk_impl(const Lattice& a, int lay, int kind, int index, float* out, long long npts, double scale,
+                            cudaStream_t st) {
+  if (lay == LAY_TWO) vtk_lay<F, LAY_TWO>(a, kind, index, out, npts, scale, st);
+  else if (lay == LAY_AAE) vtk_lay<F, LAY_AAE>(a, kind, index, out, npts, scale, st);
+  else vtk_lay<F, LAY_AAN>(a, kind, index, out, npts, scale, st);
+  return cudaGetLastError();
+}
+cudaError_t launch_vtk(const Lattice& a, int lay, int kind, int index, float* out, long long npts, double scale,
+                       cudaStream_t st) {
+  switch (a.form) {
+    case FORM_F64: return vtk_impl<F64>(a, lay, kind, index, out, npts, scale, st);
+    case FORM_F32: return vtk_impl<F32>(a, lay, kind, index, out, npts, scale, st);
+    case FORM_F16: return vtk_impl<F16>(a, lay, kind, index, out, npts, scale, st);
+  }
+  return cudaErrorInvalidValue;
 }
 
 }  // namespace bgk

@@ -99,6 +99,11 @@ cudaError_t launch_last_zj(const Lattice& a, int lay, double scale, double* out,
 cudaError_t launch_spectrum_bins(const void* fft_out, int form, int nx, int ny, int nz, int nbins, double* bins,
                                  double norm, cudaStream_t st);
 
+// Velocity float triples of a VTK slice (kind 1 xy at z = index, 2 xz at
+// y = index, 3 yz at x = index; 0-based) or of the box (kind 0), in file order.
+cudaError_t launch_vtk(const Lattice& a, int lay, int kind, int index, float* out, long long npts, double scale,
+                       cudaStream_t st);
+
 // Streaming-only calibrator (shift of three scalar fields by one cell).
 cudaError_t launch_shift3(const void* const in[3], void* const out[3], int nx, int ny, int nz, int elem_bytes,
                           int reverse, cudaStream_t st);

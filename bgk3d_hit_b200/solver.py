@@ -176,6 +176,27 @@ class BGK3D:
         check(self._lib.bgk_spectrum(self._h, nb, out.ctypes.data_as(C.POINTER(C.c_double))), "bgk_spectrum")
         return out
 
+    # ---------------------------------------------------- files (I/O)
+    def save(self, path: str):
+        """Checkpoint of the populations (restart data)."""
+        check(self._lib.bgk_save(self._h, os.fsencode(path)), "bgk_save")
+
+    def load(self, path: str):
+        check(self._lib.bgk_load(self._h, os.fsencode(path)), "bgk_load")
+
+    def vtk_xy_bin(self, itime: int, k0: int, out_dir: str = "."):
+        """= vtk_xy_bin(itime, k0) (SRC/vtk_xy.binary.F90)."""
+        check(self._lib.bgk_vtk(self._h, itime, 1, k0, os.fsencode(out_dir)), "bgk_vtk")
+
+    def vtk_xz_bin(self, itime: int, j0: int, out_dir: str = "."):
+        check(self._lib.bgk_vtk(self._h, itime, 2, j0, os.fsencode(out_dir)), "bgk_vtk")
+
+    def vtk_yz_bin(self, itime: int, i0: int, out_dir: str = "."):
+        check(self._lib.bgk_vtk(self._h, itime, 3, i0, os.fsencode(out_dir)), "bgk_vtk")
+
+    def vtk_3d_bin(self, itime: int, out_dir: str = "."):
+        check(self._lib.bgk_vtk(self._h, itime, 0, 0, os.fsencode(out_dir)), "bgk_vtk")
+
     # ------------------------------------------------------- properties
     def _getd(self, fn):
         v = C.c_double()
@@ -215,19 +236,37 @@ class BGK3D:
         check(self._lib.bgk_synchronize(self._h), "bgk_synchronize")
 
 
-def run_loop(box: BGK3D, itfin: int, out_dir: str | None = None, itstart: int = 1):
+def run_loop(box: BGK3D, itfin: int, out_dir: str | None = None, itstart: int = 1, ivtim: int | None = None,
+             itsave: int | None = None):
     """Replays the time loop of SRC/bgk3d_HIT.F90:127-146 (boundaries, col_MC,
     diagnostic) and returns the diagnostic records; with out_dir, writes
-    diagno.dat and dissipation.dat in the reference's formats (i8, e14.6)."""
+    diagno.dat and dissipation.dat in the reference's formats (i8, e14.6).
+    With ivtim, also the three mid-box VTK slices at itime 0 and on every
+    diagnostic step that is a multiple of ivtim (SRC/bgk3d_HIT.F90:118-120,
+    SRC/diagnostic.F90:52-58); with itsave, a checkpoint every itsave steps."""
+    lx, ly, lz = box.shape
     recs = []
+
+    def slices(it):
+        box.vtk_xy_bin(it, lz // 2, out_dir)
+        box.vtk_xz_bin(it, ly // 2, out_dir)
+        box.vtk_yz_bin(it, lx // 2, out_dir)
+
+    if out_dir:
+        os.makedirs(out_dir, exist_ok=True)
+        if ivtim:
+            slices(0)
     for itime in range(itstart, itfin + 1):
         box.boundaries(itime)
         box.col_MC(itime)
         d = box.diagnostic(itime)
         if d is not None:
             recs.append(d)
+            if out_dir and ivtim and itime % ivtim == 0:
+                slices(itime)
+        if out_dir and itsave and itime % itsave == 0:
+            box.save(os.path.join(out_dir, "restart.%08d.bin" % itime))
     if out_dir:
-        os.makedirs(out_dir, exist_ok=True)
         with open(os.path.join(out_dir, "diagno.dat"), "w") as f70, \
                 open(os.path.join(out_dir, "dissipation.dat"), "w") as f71:
             for d in recs:

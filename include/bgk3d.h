@@ -165,6 +165,24 @@ int bgk_get_velocity(bgk_ctx* ctx, double* u, double* v, double* w);
    k = 0..nbins-1 (cuFFT). No reference counterpart. */
 int bgk_spectrum(bgk_ctx* ctx, int nbins, double* ek);
 
+/* Checkpoint / restart of the populations (the reference reads itsave and
+   irestart, SRC/input.F90:41-42, but never saves or restarts). bgk_save
+   writes a small header (box, precision, step, scale, omega) and the 19
+   populations in the reference's meaning and order; bgk_load restores them
+   into a context of the same box and precision (either scheme) and sets its
+   step counter (and the FP16 scale). Synchronous. */
+int bgk_save(bgk_ctx* ctx, const char* path);
+int bgk_load(bgk_ctx* ctx, const char* path);
+
+/* VTK output as the reference's vtk_*_bin subroutines write it
+   (SRC/vtk_xy.binary.F90:58-97, vtk_xz / vtk_yz / vtk_3d): legacy
+   STRUCTURED_POINTS, BINARY, big-endian float32 velocity j/rho, file
+   tec_<kind>.00000.<itime, 8 digits>.vtk in `dir` (NULL: current directory).
+   kind 1: xy plane at z = index, 2: xz at y = index, 3: yz at x = index
+   (1-based, as the reference's k0, j0, i0), 0: the whole box (index ignored).
+   Synchronous. */
+int bgk_vtk(bgk_ctx* ctx, int itime, int kind, int index, const char* dir);
+
 /* Discrete adjoint of the time loop (no reference counterpart). From the
    initial velocity (u0, v0, w0) (equilibrium at rho = 1, as bgk_init_velocity),
    runs nsteps stream-collide steps with the context's omega, and computes

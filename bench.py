@@ -60,6 +60,8 @@ def parse():
     ap.add_argument("--icheck", type=int, default=100)
     ap.add_argument("--kernel", type=int, default=0, choices=[0, 1, 2, 4, 8],
                     help="stream-collide kernel (0 automatic; 2/4 cells per thread apply to FP16; 8 TMA row pipeline)")
+    ap.add_argument("--les-cs", type=float, default=0.0,
+                    help="Smagorinsky constant: > 0 times the LES collision instead of BGK")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
@@ -67,7 +69,8 @@ def parse():
 
 
 def workload_name(a):
-    return (f"decaying HIT {a.size}^3 D3Q19 BGK, {a.precision} {a.scheme}, tau={a.tau}, k0={a.k0:g}, "
+    coll = f"Smagorinsky LES cteS={a.les_cs:g}" if a.les_cs > 0 else "BGK"
+    return (f"decaying HIT {a.size}^3 D3Q19 {coll}, {a.precision} {a.scheme}, tau={a.tau}, k0={a.k0:g}, "
             f"u_rms=0.03, seed 1234")
 
 
@@ -138,6 +141,7 @@ def cpu_baseline(a, seconds: float):
 
     u, v, w = hit_velocity(L, a.k0, 0.03, 1234)
     orc.init_velocity(u, v, w, 1.0)
+    orc.set_les(a.les_cs)
     svisc = (a.tau - 0.5) / 3.0
     t1 = orc.time_steps(svisc, 1)
     steps = max(1, min(200, int(seconds / max(t1, 1e-6))))
@@ -160,6 +164,7 @@ def run_reference(a):
     orc = O.OracleLattice(L, L, L, form="f64")
     u, v, w = hit_velocity(L, a.k0, 0.03, 1234)
     orc.init_velocity(u, v, w, 1.0)
+    orc.set_les(a.les_cs)
     svisc = (a.tau - 0.5) / 3.0
     t1 = orc.time_steps(svisc, 1)
     # each timed step is a bounded sample: cap the whole run at a few minutes
@@ -219,7 +224,7 @@ def run_ours(a):
     u, v, w = hit_velocity(L, a.k0, 0.03, 1234)
     pin = [torch.from_numpy(x).pin_memory() for x in (u, v, w)]
     box = B.BGK3D(L, svisc=svisc, u0=0.03, precision=a.precision, scheme=a.scheme, icheck=a.icheck, device=local,
-                  kernel=a.kernel)
+                  kernel=a.kernel, les_cs=a.les_cs)
     box.init_velocity(*(p.numpy() for p in pin))
     stream = torch.cuda.ExternalStream(box.stream, device=local)
 
@@ -259,7 +264,7 @@ def run_ours(a):
     bpc = BYTES_PER_CELL[a.precision]
     achieved = bpc * float(L) ** 3 / per_launch_s / 1e9
     peak, peak_kind = measured_hbm()
-    kern = f"{'k_two' if a.scheme == 'two_lattice' else 'k_aa'}_{a.precision}"
+    kern = f"{'k_two' if a.scheme == 'two_lattice' else 'k_aa'}_{a.precision}" + ("_les" if a.les_cs > 0 else "")
     tr = ncu_traffic(kern)
     traffic = tr * float(L) ** 3 if tr else None
 
@@ -268,7 +273,7 @@ def run_ours(a):
     if not a.no_e2e:
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         box2 = B.BGK3D(L, svisc=svisc, u0=0.03, precision=a.precision, scheme=a.scheme, icheck=a.icheck,
-                       device=local, kernel=a.kernel)
+                       device=local, kernel=a.kernel, les_cs=a.les_cs)
         stream2 = torch.cuda.ExternalStream(box2.stream, device=local)
         torch.cuda.synchronize()
         if ws > 1:

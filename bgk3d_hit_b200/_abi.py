@@ -36,6 +36,7 @@ class BgkParams(C.Structure):
         ("precision", C.c_int), ("scheme", C.c_int), ("icheck", C.c_int), ("mode", C.c_int),
         ("fp16_scale", C.c_double), ("device", C.c_int),
         ("use_omega", C.c_int), ("omega", C.c_double), ("extras", C.c_int), ("kernel", C.c_int),
+        ("les_cs", C.c_double),
     ]
 
 

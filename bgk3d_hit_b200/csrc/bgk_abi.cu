@@ -270,6 +270,7 @@ int bgk_params_default(bgk_params* p) {
   p->omega = 0.0;
   p->extras = 1;
   p->kernel = 0;
+  p->les_cs = 0.0;
   return BGK_OK;
 }
 
@@ -299,6 +300,10 @@ int bgk_create(const bgk_params* p, bgk_ctx** out) {
   }
   if (p->kernel != 0 && p->kernel != 1 && p->kernel != 2 && p->kernel != 4 && p->kernel != 8) {
     set_err("kernel must be 0, 1, 2, 4 or 8 (got %d)", p->kernel);
+    return BGK_ERR_INVALID;
+  }
+  if (!(p->les_cs >= 0.0 && p->les_cs <= 10.0)) {
+    set_err("les_cs must be a Smagorinsky constant in [0, 10] (got %g)", p->les_cs);
     return BGK_ERR_INVALID;
   }
   if (p->icheck < 1) {
@@ -505,7 +510,7 @@ int bgk_col_mc(bgk_ctx* c, int itime) {
   if (rc) return rc;
   CK(cudaSetDevice(c->p.device));
   if (c->scheme == BGK_TWO_LATTICE) {
-    CK(launch_two_lattice(c->A, c->B, c->omega, c->scale, c->p.kernel, c->st));
+    CK(launch_two_lattice(c->A, c->B, c->omega, c->scale, c->p.les_cs, c->p.kernel, c->st));
     // pointer swap of pops 01..18, SRC/col_MC.F90:364-421
     for (int q = 0; q < Q - 1; ++q) {
       void* t = c->A.p[q];
@@ -514,7 +519,7 @@ int bgk_col_mc(bgk_ctx* c, int itime) {
     }
   } else {
     const int odd = c->lay == LAY_AAE;
-    CK(launch_aa(c->A, odd, c->omega, c->scale, c->p.kernel, c->st));
+    CK(launch_aa(c->A, odd, c->omega, c->scale, c->p.les_cs, c->p.kernel, c->st));
     c->lay = odd ? LAY_AAN : LAY_AAE;
   }
   c->launches++;
@@ -526,8 +531,8 @@ int bgk_col_mc(bgk_ctx* c, int itime) {
 int bgk_debug_stall_next_step(bgk_ctx* c) {
   int rc = check_ctx(c);
   if (rc) return rc;
-  if (c->p.kernel != 8) {
-    set_err("bgk_debug_stall_next_step needs the row-pipelined kernel (params.kernel = 8)");
+  if (c->p.kernel != 8 || c->p.les_cs > 0.0) {
+    set_err("bgk_debug_stall_next_step needs the row-pipelined kernel (params.kernel = 8, BGK collision)");
     return BGK_ERR_INVALID;
   }
   c->A.stall = c->B.stall = 1;
@@ -929,6 +934,10 @@ int adj_check(bgk_ctx* c, int nsteps) {
   if (rc) return rc;
   if (c->form == FORM_F16) {
     set_err("the adjoint and tangent models support the FP64 and FP32 forms");
+    return BGK_ERR_INVALID;
+  }
+  if (c->p.les_cs > 0.0) {
+    set_err("the adjoint and tangent models differentiate the BGK collision (les_cs must be 0)");
     return BGK_ERR_INVALID;
   }
   if (nsteps < 1) {

@@ -55,7 +55,7 @@ static int grid_1d(long long n, int threads, int cap) {
 }
 
 // ------------------------------------------------------------- two lattice
-template <class F>
+template <class F, bool LES = false>
 __global__ void __launch_bounds__(256) k_two(Pops<const typename F::S> src, Pops<typename F::S> dst, Geo g, StepK K) {
   using S = typename F::S;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -77,7 +77,7 @@ __global__ void __launch_bounds__(256) k_two(Pops<const typename F::S> src, Pops
     // (src.p[18] == dst.p[18]); the adjoint's out-of-place steps pass distinct arrays
     v[q] = (q == Q - 1) ? src.p[Q - 1][off] : ldg(src.p[q] + off);
   }
-  F::cell(v, K);
+  F::template cell<LES>(v, K);
   const int o = i + g.sx * (j + g.ny * k);
 #pragma unroll
   for (int q = 0; q < Q; ++q) dst.p[q][o] = v[q];
@@ -253,7 +253,7 @@ __global__ void __launch_bounds__(256, 4) k_two_f16v2(Pops<const __half> src, Po
 // Each thread reads exactly the locations it writes, so the update is
 // race-free in place; a location is never read after it has been written,
 // which also makes the read-only load path safe.
-template <class F, bool ODD>
+template <class F, bool ODD, bool LES = false>
 __global__ void __launch_bounds__(256) k_aa(Pops<typename F::S> a, Geo g, StepK K) {
   using S = typename F::S;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -274,7 +274,7 @@ __global__ void __launch_bounds__(256) k_aa(Pops<typename F::S> a, Geo g, StepK 
   S v[Q];
 #pragma unroll
   for (int q = 0; q < Q; ++q) v[q] = ODD ? ldg(a.p[oppq(q)] + back(q)) : ldg(a.p[q] + o);
-  F::cell(v, K);
+  F::template cell<LES>(v, K);
 #pragma unroll
   for (int q = 0; q < Q; ++q) {
     if (ODD) a.p[q][back(oppq(q))] = v[q];
@@ -633,14 +633,28 @@ template <class S> static Pops<S> pops_of(const Lattice& L) {
   return p;
 }
 
-StepK make_stepk(int form, double omega, double scale) {
+StepK make_stepk(int form, double omega, double scale, double les_cs) {
   StepK k{};
   k.omega = omega;
   k.omega_f = (float)omega;
   k.inv = (float)(1.0 / scale);
   k.om1 = 1.0f - (float)omega;
+  k.scale = (float)scale;
   const double w[3] = {1.0 / 3.0, 1.0 / 18.0, 1.0 / 36.0};
   for (int c = 0; c < 3; ++c) k.kw[c] = (float)((double)(float)omega * scale * w[c]);
+  // Smagorinsky constants of SRC/col_MC.F90:305 in the form's arithmetic:
+  // 18*(cteS)**2, 1/(2*omega1) and (1/omega1)**2 (host code is built without
+  // contraction, so each operation rounds as written)
+  k.les = les_cs > 0.0;
+  if (k.les) {
+    k.cs18 = 18.0 * (les_cs * les_cs);
+    k.tauh = 1.0 / (2.0 * omega);
+    k.tau2 = (1.0 / omega) * (1.0 / omega);
+    const float cs = (float)les_cs, om = (float)omega;
+    k.cs18_f = 18.0f * (cs * cs);
+    k.tauh_f = 1.0f / (2.0f * om);
+    k.tau2_f = (1.0f / om) * (1.0f / om);
+  }
   (void)form;
   return k;
 }
@@ -662,6 +676,11 @@ static cudaError_t two_impl(const Lattice& s, const Lattice& d, const StepK& K, 
   Pops<const S> ps = pops_of<const S>(s);
   Pops<S> pd = pops_of<S>(d);
   pd.p[Q - 1] = (S*)s.p[Q - 1];  // pop 19 in place (SRC/col_MC.F90:351)
+  Shape sh = cell_shape(s.g);
+  if (K.les) {  // the Smagorinsky collision runs on the one cell per thread kernel
+    k_two<F, true><<<sh.grid, sh.block, 0, st>>>(ps, pd, s.g, K);
+    return cudaGetLastError();
+  }
   if (variant == 8) {
     bool launched = false;
     cudaError_t e = launch_rows(s, d, ROW_TWO, K, st, &launched);
@@ -683,7 +702,6 @@ static cudaError_t two_impl(const Lattice& s, const Lattice& d, const StepK& K, 
       return cudaGetLastError();
     }
   }
-  Shape sh = cell_shape(s.g);
   k_two<F><<<sh.grid, sh.block, 0, st>>>(ps, pd, s.g, K);
   return cudaGetLastError();
 }
@@ -702,9 +720,9 @@ cudaError_t launch_step_out_of_place(const Lattice& src, const Lattice& dst, dou
   return cudaErrorInvalidValue;
 }
 
-cudaError_t launch_two_lattice(const Lattice& src, const Lattice& dst, double omega, double scale, int variant,
-                               cudaStream_t st) {
-  const StepK K = make_stepk(src.form, omega, scale);
+cudaError_t launch_two_lattice(const Lattice& src, const Lattice& dst, double omega, double scale, double les_cs,
+                               int variant, cudaStream_t st) {
+  const StepK K = make_stepk(src.form, omega, scale, les_cs);
   switch (src.form) {
     case FORM_F64: return two_impl<F64>(src, dst, K, variant, st);
     case FORM_F32: return two_impl<F32>(src, dst, K, variant, st);
@@ -716,19 +734,25 @@ cudaError_t launch_two_lattice(const Lattice& src, const Lattice& dst, double om
 template <class F>
 static cudaError_t aa_impl(const Lattice& a, int odd, const StepK& K, int variant, cudaStream_t st) {
   using S = typename F::S;
+  Shape sh = cell_shape(a.g);
+  if (K.les) {
+    if (odd) k_aa<F, true, true><<<sh.grid, sh.block, 0, st>>>(pops_of<S>(a), a.g, K);
+    else k_aa<F, false, true><<<sh.grid, sh.block, 0, st>>>(pops_of<S>(a), a.g, K);
+    return cudaGetLastError();
+  }
   if (variant == 8) {
     bool launched = false;
     cudaError_t e = launch_rows(a, a, odd ? ROW_AA_ODD : ROW_AA_EVEN, K, st, &launched);
     if (e != cudaSuccess || launched) return e;
   }
-  Shape sh = cell_shape(a.g);
   if (odd) k_aa<F, true><<<sh.grid, sh.block, 0, st>>>(pops_of<S>(a), a.g, K);
   else k_aa<F, false><<<sh.grid, sh.block, 0, st>>>(pops_of<S>(a), a.g, K);
   return cudaGetLastError();
 }
 
-cudaError_t launch_aa(const Lattice& a, int odd, double omega, double scale, int variant, cudaStream_t st) {
-  const StepK K = make_stepk(a.form, omega, scale);
+cudaError_t launch_aa(const Lattice& a, int odd, double omega, double scale, double les_cs, int variant,
+                      cudaStream_t st) {
+  const StepK K = make_stepk(a.form, omega, scale, les_cs);
   switch (a.form) {
     case FORM_F64: return aa_impl<F64>(a, odd, K, variant, st);
     case FORM_F32: return aa_impl<F32>(a, odd, K, variant, st);

@@ -30,14 +30,14 @@ constexpr int DIAG_BLOCKS = 148 * 4;
 constexpr int DIAG_THREADS = 256;
 
 // Collision constants of one launch for a form.
-StepK make_stepk(int form, double omega, double scale);
+StepK make_stepk(int form, double omega, double scale, double les_cs = 0.0);
 
 // Two-lattice fused pull-stream + collide: src -> dst (pops 1..18), pop 19 in
 // place in src. variant: 0 automatic, 1 one cell per thread, 2 / 4 cells per
 // thread for the FP16 form, 8 row pipeline with TMA bulk copies (each falls
 // back to 1 where the box does not fit it).
-cudaError_t launch_two_lattice(const Lattice& src, const Lattice& dst, double omega, double scale, int variant,
-                               cudaStream_t st);
+cudaError_t launch_two_lattice(const Lattice& src, const Lattice& dst, double omega, double scale, double les_cs,
+                               int variant, cudaStream_t st);
 // One step src -> dst with all 19 populations written to dst (pop 19 too);
 // FP64 and FP32 forms (used by the adjoint's recomputation).
 cudaError_t launch_step_out_of_place(const Lattice& src, const Lattice& dst, double omega, cudaStream_t st);
@@ -67,7 +67,8 @@ cudaError_t launch_acc_total(const double* acc, double* total, cudaStream_t st);
 
 // AA pattern: even (local read, reversed local write) or odd (pull from
 // neighbours' opposite slots, push to neighbours). variant as above (1 or 8).
-cudaError_t launch_aa(const Lattice& a, int odd, double omega, double scale, int variant, cudaStream_t st);
+cudaError_t launch_aa(const Lattice& a, int odd, double omega, double scale, double les_cs, int variant,
+                      cudaStream_t st);
 // Row-pipelined kernel; *launched = false when the box does not fit it.
 cudaError_t launch_rows(const Lattice& src, const Lattice& dst, int mode, const StepK& K, cudaStream_t st,
                         bool* launched);

@@ -47,6 +47,8 @@ __device__ __forceinline__ Ex<float> operator-(Ex<float> a, Ex<float> b) { retur
 __device__ __forceinline__ Ex<float> operator*(Ex<float> a, Ex<float> b) { return {__fmul_rn(a.v, b.v)}; }
 __device__ __forceinline__ Ex<float> operator/(Ex<float> a, Ex<float> b) { return {__fdiv_rn(a.v, b.v)}; }
 template <class T> __device__ __forceinline__ Ex<T> operator-(Ex<T> a) { return {-a.v}; }
+__device__ __forceinline__ Ex<double> esqrt(Ex<double> a) { return {__dsqrt_rn(a.v)}; }
+__device__ __forceinline__ Ex<float> esqrt(Ex<float> a) { return {__fsqrt_rn(a.v)}; }
 
 template <class V> struct Num;  // constants and conversions for V
 template <> struct Num<double> {
@@ -76,6 +78,13 @@ struct StepK {
   float inv;      // F16: 1/scale
   float om1;      // F16: 1 - omega
   float kw[3];    // F16: omega*scale*w for w = 1/3, 1/18, 1/36
+  // Smagorinsky closure (SRC/col_MC.F90:221-309): les != 0 enables it;
+  // cs18 = 18*cteS^2, tauh = 1/(2*omega), tau2 = (1/omega)^2, in double (F64)
+  // and float (F32, F16) arithmetic
+  int les;
+  double cs18, tauh, tau2;
+  float cs18_f, tauh_f, tau2_f;
+  float scale;    // F16: scale
 };
 
 // Weight class of population q: 0 -> 1/3 (rest), 1 -> 1/18, 2 -> 1/36.
@@ -85,6 +94,8 @@ __host__ __device__ constexpr int wclass(int q) {
 
 template <class V>
 __device__ __forceinline__ void collide(V (&x)[Q], V omega);
+template <class V>
+__device__ __forceinline__ void collide_les(V (&x)[Q], V cs18, V tauh, V tau2);
 
 // F64: double storage / double arithmetic (reference DOUBLE_P build).
 // F32: float storage of f - w / float arithmetic (reference default build).
@@ -94,11 +105,13 @@ struct F64 {
   static constexpr int id = 0;
   __device__ static __forceinline__ R dec(S s, R) { return s; }
   __device__ static __forceinline__ S enc(R r, R) { return r; }
+  template <bool LES = false>
   __device__ static __forceinline__ void cell(S (&s)[Q], const StepK& k) {
     V x[Q];
 #pragma unroll
     for (int q = 0; q < Q; ++q) x[q] = V{s[q]};
-    collide<V>(x, V{k.omega});
+    if constexpr (LES) collide_les<V>(x, V{k.cs18}, V{k.tauh}, V{k.tau2});
+    else collide<V>(x, V{k.omega});
 #pragma unroll
     for (int q = 0; q < Q; ++q) s[q] = x[q].v;
   }
@@ -108,11 +121,13 @@ struct F32 {
   static constexpr int id = 1;
   __device__ static __forceinline__ R dec(S s, R) { return s; }
   __device__ static __forceinline__ S enc(R r, R) { return r; }
+  template <bool LES = false>
   __device__ static __forceinline__ void cell(S (&s)[Q], const StepK& k) {
     V x[Q];
 #pragma unroll
     for (int q = 0; q < Q; ++q) x[q] = V{s[q]};
-    collide<V>(x, V{k.omega_f});
+    if constexpr (LES) collide_les<V>(x, V{k.cs18_f}, V{k.tauh_f}, V{k.tau2_f});
+    else collide<V>(x, V{k.omega_f});
 #pragma unroll
     for (int q = 0; q < Q; ++q) s[q] = x[q].v;
   }
@@ -128,7 +143,7 @@ struct F32 {
 //     Q2 = (4.5 cu) cu + a,  P(+-) = +-3 cu + Q2   (f_eq/w - 1 = dr + (1+dr) P)
 //   y' = (1 - omega) y + kd + kr P, kd = K dr, kr = K + kd, K = omega*scale*w.
 // Sums and roundings are fixed (moments16, pair16) and restated by the oracle.
-struct Mom16 { float ux, uy, uz, a, kd[3], kr[3]; };
+struct Mom16 { float dr, ux, uy, uz, a, kd[3], kr[3]; };
 
 __device__ __forceinline__ Mom16 moments16(const float (&y)[Q], const StepK& k) {
   const float sp = __fadd_rn(__fadd_rn(__fadd_rn(y[0], y[1]), __fadd_rn(y[2], y[3])), y[4]);
@@ -144,6 +159,7 @@ __device__ __forceinline__ Mom16 moments16(const float (&y)[Q], const StepK& k) 
   const float jzm = __fadd_rn(__fadd_rn(__fadd_rn(y[1], y[8]), __fadd_rn(y[10], y[14])), y[15]);
   Mom16 m;
   const float dr = __fmul_rn(sum, k.inv);
+  m.dr = dr;
   const float r = __fdiv_rn(k.inv, __fadd_rn(1.0f, dr));
   m.ux = __fmul_rn(jx, r);
   m.uy = __fmul_rn(__fsub_rn(jyp, jym), r);
@@ -185,16 +201,59 @@ __device__ __forceinline__ float rest16(float y, const Mom16& m, float om1) {
   return __fmaf_rn(m.kr[0], m.a, __fmaf_rn(om1, y, m.kd[0]));
 }
 
+// FP16 form with the Smagorinsky closure: per cell, Pi_neq from the
+// non-equilibrium n_q = y_q/scale - w_q (dr + (1 + dr) P_q), Ptotal =
+// sqrt(Pi:Pi), tau = tauh + sqrt(cs18 Ptotal + tau2)/2 and the relaxation
+// y' = (1 - omega_eff) y + omega_eff scale w (dr + (1 + dr) P).
+__device__ __forceinline__ void cell16_les(const float (&y)[Q], __half (&s)[Q], const StepK& k) {
+  const Mom16 m = moments16(y, k);
+  const float dr = m.dr;
+  float t[Q], nn[Q];
+#pragma unroll
+  for (int q = 0; q < Q; ++q) {
+    const float cu = cdotu(q, m);
+    const float P = __fmaf_rn(3.0f, cu, __fmaf_rn(__fmul_rn(4.5f, cu), cu, m.a));
+    t[q] = __fmaf_rn(dr, P, __fadd_rn(dr, P));
+    const float w = wclass(q) == 0 ? 1.0f / 3.0f : (wclass(q) == 1 ? 1.0f / 18.0f : 1.0f / 36.0f);
+    nn[q] = __fsub_rn(__fmul_rn(y[q], k.inv), __fmul_rn(w, t[q]));
+  }
+  const float Pxx = nn[0] + nn[1] + nn[2] + nn[3] + nn[4] + nn[9] + nn[10] + nn[11] + nn[12] + nn[13];
+  const float Pyy = nn[0] + nn[2] + nn[6] + nn[7] + nn[8] + nn[9] + nn[11] + nn[15] + nn[16] + nn[17];
+  const float Pzz = nn[1] + nn[3] + nn[5] + nn[6] + nn[8] + nn[10] + nn[12] + nn[14] + nn[15] + nn[17];
+  const float Pxz = -nn[1] + nn[3] + nn[10] - nn[12];
+  const float Pxy = -nn[0] + nn[2] + nn[9] - nn[11];
+  const float Pyz = nn[6] - nn[8] + nn[15] - nn[17];
+  float pt = __fmul_rn(Pxx, Pxx);
+  pt = __fmaf_rn(Pyy, Pyy, pt);
+  pt = __fmaf_rn(Pzz, Pzz, pt);
+  pt = __fmaf_rn(2.0f * Pxy, Pxy, pt);
+  pt = __fmaf_rn(2.0f * Pxz, Pxz, pt);
+  pt = __fmaf_rn(2.0f * Pyz, Pyz, pt);
+  const float tau = __fadd_rn(k.tauh_f, __fmul_rn(0.5f, __fsqrt_rn(__fmaf_rn(k.cs18_f, __fsqrt_rn(pt), k.tau2_f))));
+  const float om = __fdiv_rn(1.0f, tau);
+  const float om1 = __fsub_rn(1.0f, om);
+#pragma unroll
+  for (int q = 0; q < Q; ++q) {
+    const float w = wclass(q) == 0 ? 1.0f / 3.0f : (wclass(q) == 1 ? 1.0f / 18.0f : 1.0f / 36.0f);
+    s[q] = __float2half_rn(__fmaf_rn(__fmul_rn(__fmul_rn(om, k.scale), w), t[q], __fmul_rn(om1, y[q])));
+  }
+}
+
 struct F16 {
   using S = __half; using R = float; using V = Ex<float>;
   static constexpr int id = 2;
   // inv and scale are exact powers of two: the multiply only moves the exponent
   __device__ static __forceinline__ R dec(S s, R inv) { return __fmul_rn(__half2float(s), inv); }
   __device__ static __forceinline__ S enc(R r, R scale) { return __float2half_rn(__fmul_rn(r, scale)); }
+  template <bool LES = false>
   __device__ static __forceinline__ void cell(S (&s)[Q], const StepK& k) {
     float y[Q];
 #pragma unroll
     for (int q = 0; q < Q; ++q) y[q] = __half2float(s[q]);
+    if constexpr (LES) {
+      cell16_les(y, s, k);
+      return;
+    }
     const Mom16 m = moments16(y, k);
 #pragma unroll
     for (int q = 0; q < 9; ++q) {
@@ -279,6 +338,25 @@ template <class V>
 __device__ __forceinline__ void collide(V (&x)[Q], V omega) {
   V e[Q], vx, vy, vz;
   (void)equilibrium<V>(x, e, vx, vy, vz);
+#pragma unroll
+  for (int q = 0; q < Q; ++q) x[q] = x[q] - omega * (x[q] - e[q]);
+}
+
+template <class V>
+__device__ __forceinline__ V ptotal(const V (&x)[Q], const V (&e)[Q]);
+
+// Smagorinsky relaxation of the reference's LES block (SRC/col_MC.F90:221-309,
+// disabled there by a stop): Ptotal = sqrt(Pi_neq:Pi_neq),
+// Ts = 1/(2 omega1) + sqrt(18 cteS^2 Ptotal + (1/omega1)^2)/2, omega = 1/Ts,
+// then the BGK update with that omega.
+template <class V>
+__device__ __forceinline__ void collide_les(V (&x)[Q], V cs18, V tauh, V tau2) {
+  using N = Num<V>;
+  V e[Q], vx, vy, vz;
+  (void)equilibrium<V>(x, e, vx, vy, vz);
+  const V pt = esqrt(ptotal<V>(x, e));
+  const V ts = tauh + esqrt(cs18 * pt + tau2) / N::c(2.0);
+  const V omega = N::c(1.0) / ts;
 #pragma unroll
   for (int q = 0; q < Q; ++q) x[q] = x[q] - omega * (x[q] - e[q]);
 }

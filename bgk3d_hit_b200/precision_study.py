@@ -1,7 +1,7 @@
 """Accuracy of the FP32 and FP16 storage forms against FP64 on decaying HIT.
 
     python -m bgk3d_hit_b200.precision_study [--size 512] [--steps 5000] [--every 100]
-        [--k0 6] [--tau 0.503] [--scheme two_lattice] [--out results.json]
+        [--k0 6] [--tau 0.503] [--scheme two_lattice] [--les-cs 0] [--out results.json]
 
 Runs the same seeded HIT initial condition (random-phase solenoidal field,
 E(k) ~ k^4 exp(-2 (k/k0)^2), u_rms = 0.03) in the three storage forms side by
@@ -16,6 +16,9 @@ Plain BGK is unstable when the flow becomes under-resolved at low viscosity
 (tau close to 1/2): a form whose diagnostics turn non-finite is stopped, its
 blow-up step is reported, and the errors are taken over the steps at which
 every form was still finite (the spectrum then at the last such record).
+With --les-cs C > 0 every form runs the Smagorinsky collision (cteS = C,
+SRC/col_MC.F90:221-309), which keeps such runs finite; eps then still uses
+the molecular viscosity.
 """
 from __future__ import annotations
 
@@ -33,14 +36,15 @@ FORMS = ("fp64", "fp32", "fp16")
 
 
 def run(size=512, steps=5000, every=100, k0=6.0, tau=0.503, u_rms=0.03, seed=1234, scheme="two_lattice",
-        forms=FORMS, device=0):
+        forms=FORMS, device=0, les_cs=0.0):
     svisc = (tau - 0.5) / 3.0
     t0 = time.time()
     u, v, w = hit_velocity(size, k0, u_rms, seed)
     t_ic = time.time() - t0
     boxes = {}
     for f in forms:
-        b = BGK3D(size, svisc=svisc, u0=u_rms, precision=f, scheme=scheme, icheck=every, device=device)
+        b = BGK3D(size, svisc=svisc, u0=u_rms, precision=f, scheme=scheme, icheck=every, device=device,
+                  les_cs=les_cs)
         b.init_velocity(u, v, w)
         boxes[f] = b
     del u, v, w
@@ -94,7 +98,7 @@ def run(size=512, steps=5000, every=100, k0=6.0, tau=0.503, u_rms=0.03, seed=123
     ref = series["fp64"] if "fp64" in series else None
     common = min(len(series[f]["step"]) for f in forms)  # records where every form was finite
     out = {"config": {"size": size, "steps": steps, "every": every, "k0": k0, "tau": tau, "u_rms": u_rms,
-                      "seed": seed, "scheme": scheme},
+                      "seed": seed, "scheme": scheme, "les_cs": les_cs},
            "seconds": {"initial_condition": t_ic, "run": t_run},
            "compared_up_to_step": series[forms[0]]["step"][common - 1],
            "spectrum_step": next(iter(spec.values()))[0] if spec else None, "forms": {}}
@@ -129,9 +133,10 @@ def main():
     ap.add_argument("--k0", type=float, default=6.0)
     ap.add_argument("--tau", type=float, default=0.503)
     ap.add_argument("--scheme", default="two_lattice")
+    ap.add_argument("--les-cs", type=float, default=0.0, help="Smagorinsky constant (0: BGK)")
     ap.add_argument("--out", default=None, help="write the full series and spectra here (JSON)")
     a = ap.parse_args()
-    res = run(a.size, a.steps, a.every, a.k0, a.tau, scheme=a.scheme)
+    res = run(a.size, a.steps, a.every, a.k0, a.tau, scheme=a.scheme, les_cs=a.les_cs)
     if a.out:
         with open(a.out, "w") as f:
             json.dump(res, f)

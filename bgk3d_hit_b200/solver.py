@@ -54,7 +54,7 @@ class BGK3D:
     def __init__(self, lx: int = 64, ly: int | None = None, lz: int | None = None, *, svisc: float = 0.01,
                  u0: float = 0.05, precision: str = "fp64", scheme: str = "two_lattice", icheck: int = 10,
                  mode: str = "corrected", fp16_scale: float = 0.0, device: int = 0, omega: float | None = None,
-                 extras: bool = True, kernel: int = 0):
+                 extras: bool = True, kernel: int = 0, les_cs: float = 0.0):
         self._lib = _abi.load()
         p = BgkParams()
         check(self._lib.bgk_params_default(C.byref(p)), "bgk_params_default")
@@ -64,6 +64,7 @@ class BGK3D:
         p.scheme = _abi.SCHEMES[scheme] if isinstance(scheme, str) else int(scheme)
         p.mode = _abi.MODES[mode] if isinstance(mode, str) else int(mode)
         p.icheck, p.fp16_scale, p.device, p.extras, p.kernel = icheck, fp16_scale, device, int(extras), kernel
+        p.les_cs = les_cs
         if omega is not None:
             p.use_omega, p.omega = 1, omega
         self.params = p

@@ -85,6 +85,14 @@ typedef struct {
                           pipeline with TMA bulk copies into shared memory (rows up to
                           about 5 KB); boxes a kernel does not fit use 1. All give
                           identical results. */
+  double les_cs;       /* Smagorinsky constant cteS (SRC/input.F90:47, SRC/storage.F90:87).
+                          > 0 enables the LES collision of SRC/col_MC.F90:221-309 (the
+                          block the reference compiles under -DLES and then stops in):
+                          per cell Ptotal = |Pi_neq|, Ts = 1/(2 omega) +
+                          sqrt(18 cteS^2 Ptotal + (1/omega)^2)/2, relaxation with 1/Ts.
+                          0 (default) = plain BGK. The LES collision runs on the one
+                          cell per thread kernels (kernel 2/4/8 fall back to them);
+                          bgk_adjoint and bgk_tangent reject it. */
 } bgk_params;
 
 /* Diagnostics of one step, in FP64. */

@@ -34,6 +34,7 @@
 #define REAL double
 #define SIN sin
 #define COS cos
+#define SQRT sqrt
 #define ENC(L, x) (x)
 #define DEC(L, s) (s)
 #include "bgk_oracle_impl.h"
@@ -42,6 +43,7 @@
 #undef REAL
 #undef SIN
 #undef COS
+#undef SQRT
 #undef ENC
 #undef DEC
 
@@ -50,6 +52,7 @@
 #define REAL float
 #define SIN sinf
 #define COS cosf
+#define SQRT sqrtf
 #define ENC(L, x) (x)
 #define DEC(L, s) (s)
 #include "bgk_oracle_impl.h"
@@ -58,6 +61,7 @@
 #undef REAL
 #undef SIN
 #undef COS
+#undef SQRT
 #undef ENC
 #undef DEC
 
@@ -67,6 +71,7 @@
 #define REAL float
 #define SIN sinf
 #define COS cosf
+#define SQRT sqrtf
 #define ENC(L, x) ((_Float16)((x) * (L)->scale))
 #define DEC(L, s) ((float)(s) * (L)->inv_scale)
 #include "bgk_oracle_impl.h"
@@ -76,6 +81,7 @@
 #undef REAL
 #undef SIN
 #undef COS
+#undef SQRT
 #undef ENC
 #undef DEC
 

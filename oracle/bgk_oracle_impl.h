@@ -15,6 +15,7 @@
  *   SUF        symbol suffix (_f64, _f32, _f16)
  *   STOR       storage type of a population value
  *   REAL       arithmetic type (mykind in SRC/precision.F90:19-38)
+ *   SIN, COS, SQRT  REAL math functions
  *   ENC(L,x)   REAL deviation -> stored value
  *   DEC(L,s)   stored value -> REAL deviation
  *
@@ -37,6 +38,7 @@ typedef struct {
     STOR *a[19];
     STOR *b[19];
     REAL scale, inv_scale;
+    double les_cs; /* Smagorinsky constant cteS; 0 = BGK collision */
 } LAT;
 
 static inline long FN(gidx)(const LAT *L, long i, long j, long k) {
@@ -65,6 +67,12 @@ void FN(orc_destroy)(LAT *L) {
     if (!L) return;
     for (int q = 0; q < 19; ++q) { free(L->a[q]); free(L->b[q]); }
     free(L);
+}
+
+/* Selects the LES collision of SRC/col_MC.F90:221-309 with cteS = cs
+   (cs > 0) or the plain BGK collision (cs = 0). */
+void FN(orc_set_les)(LAT *L, double cs) {
+    L->les_cs = cs;
 }
 
 void FN(orc_set_scale)(LAT *L, double scale) {
@@ -340,7 +348,60 @@ static void FN(fast16_cell)(const float *y, float *out, float inv, float om1, co
     }
     out[18] = fmaf(kr[0], a, fmaf(om1, y[18], kd[0]));
 }
+
+/* The FP16 form with the Smagorinsky closure (the reference's LES block,
+   SRC/col_MC.F90:221-309, on the FP16 form's moments): with dr, u and a as in
+   fast16_cell and P_q = fmaf(3, cu, fmaf(4.5*cu, cu, a)),
+     t_q = fmaf(dr, P_q, dr + P_q)               (f_eq/w - 1)
+     n_q = y_q*inv - w_q*t_q                      (non-equilibrium, unscaled)
+     Pij from n as in FN(ptotal), pt = Pxx^2 (+ fmaf chain of the others),
+     tau = tauh + 0.5*sqrt(fmaf(cs18, sqrt(pt), tau2)), om = 1/tau,
+     y'_q = fmaf(om*scale*w_q, t_q, (1 - om)*y_q). */
+static void FN(fast16_les_cell)(const float *y, float *out, float inv, float scale, float cs18, float tauh,
+                                float tau2) {
+    static const int wcls[19] = {2,2,2,2,1,1,2,1,2,2,2,2,2,1,1,2,1,2,0};
+    const float wv[3] = {1.0f / 3.0f, 1.0f / 18.0f, 1.0f / 36.0f};
+    const float sp = ((y[0] + y[1]) + (y[2] + y[3])) + y[4];
+    const float sm = ((y[9] + y[10]) + (y[11] + y[12])) + y[13];
+    const float s0 = (((y[5] + y[6]) + (y[7] + y[8])) + ((y[14] + y[15]) + (y[16] + y[17]))) + y[18];
+    const float sum = (sp + sm) + s0;
+    const float jx = sp - sm;
+    const float jyp = ((y[2] + y[6]) + (y[7] + y[8])) + y[11];
+    const float jym = ((y[0] + y[9]) + (y[15] + y[16])) + y[17];
+    const float jzp = ((y[3] + y[5]) + (y[6] + y[12])) + y[17];
+    const float jzm = ((y[1] + y[8]) + (y[10] + y[14])) + y[15];
+    const float dr = sum * inv;
+    const float r = inv / (1.0f + dr);
+    const float ux = jx * r, uy = (jyp - jym) * r, uz = (jzp - jzm) * r;
+    const float usq = fmaf(uz, uz, fmaf(uy, uy, ux * ux));
+    const float a = -1.5f * usq;
+    float t[19], nn[19];
+    for (int q = 0; q < 19; ++q) {
+        const float cu = q == 18 ? 0.0f : FN(cdotu16)(q, ux, uy, uz);
+        const float P = fmaf(3.0f, cu, fmaf(4.5f * cu, cu, a));
+        t[q] = fmaf(dr, P, dr + P);
+        nn[q] = y[q] * inv - wv[wcls[q]] * t[q];
+    }
+    const float Pxx = nn[0] + nn[1] + nn[2] + nn[3] + nn[4] + nn[9] + nn[10] + nn[11] + nn[12] + nn[13];
+    const float Pyy = nn[0] + nn[2] + nn[6] + nn[7] + nn[8] + nn[9] + nn[11] + nn[15] + nn[16] + nn[17];
+    const float Pzz = nn[1] + nn[3] + nn[5] + nn[6] + nn[8] + nn[10] + nn[12] + nn[14] + nn[15] + nn[17];
+    const float Pxz = -nn[1] + nn[3] + nn[10] - nn[12];
+    const float Pxy = -nn[0] + nn[2] + nn[9] - nn[11];
+    const float Pyz = nn[6] - nn[8] + nn[15] - nn[17];
+    float pt = Pxx * Pxx;
+    pt = fmaf(Pyy, Pyy, pt);
+    pt = fmaf(Pzz, Pzz, pt);
+    pt = fmaf(2.0f * Pxy, Pxy, pt);
+    pt = fmaf(2.0f * Pxz, Pxz, pt);
+    pt = fmaf(2.0f * Pyz, Pyz, pt);
+    const float tau = tauh + 0.5f * sqrtf(fmaf(cs18, sqrtf(pt), tau2));
+    const float om = 1.0f / tau;
+    const float om1 = 1.0f - om;
+    for (int q = 0; q < 19; ++q) out[q] = fmaf((om * scale) * wv[wcls[q]], t[q], om1 * y[q]);
+}
 #endif
+
+static inline REAL FN(ptotal)(const REAL x[19], const REAL e[19]);
 
 /* One fused pull-stream + BGK collide over the interior followed by the swap
    of pops 01..18, SRC/col_MC.F90:98-421. omega is passed in REAL precision.
@@ -348,6 +409,13 @@ static void FN(fast16_cell)(const float *y, float *out, float inv, float om1, co
 void FN(orc_col_mc_omega)(LAT *L, double omegad, int periodic) {
     const REAL omega = (REAL)omegad;
     const long l = L->l, m = L->m, n = L->n;
+    /* LES constants of SRC/col_MC.F90:305 in REAL arithmetic:
+       18*(cteS)**2, 1/(2*omega1), (1/omega1)**2 */
+    const int les = L->les_cs > 0.0;
+    const REAL cs = (REAL)L->les_cs;
+    const REAL cs18 = (REAL)18 * (cs * cs);
+    const REAL tauh = (REAL)1 / ((REAL)2 * omega);
+    const REAL tau2 = ((REAL)1 / omega) * ((REAL)1 / omega);
 #ifdef FAST16
     const float inv = (float)L->inv_scale, om1 = 1.0f - (float)omega;
     const double wd[3] = {1.0 / 3.0, 1.0 / 18.0, 1.0 / 36.0};
@@ -370,15 +438,23 @@ void FN(orc_col_mc_omega)(LAT *L, double omegad, int periodic) {
                     }
                     y[q] = (float)L->a[q][FN(gidx)(L, si, sj, sk)];
                 }
-                FN(fast16_cell)(y, out, inv, om1, kw);
+                if (les) FN(fast16_les_cell)(y, out, inv, (float)L->scale, cs18, tauh, tau2);
+                else FN(fast16_cell)(y, out, inv, om1, kw);
                 for (int q = 0; q < 18; ++q) L->b[q][g] = (STOR)out[q];
                 L->a[18][g] = (STOR)out[18];
 #else
                 REAL x[19], e[19], ux, uy, uz;
                 FN(pull)(L, L->a, i, j, k, periodic, x);
                 (void)FN(equilibrium)(x, e, &ux, &uy, &uz);
-                for (int q = 0; q < 18; ++q) L->b[q][g] = ENC(L, x[q] - omega * (x[q] - e[q]));
-                L->a[18][g] = ENC(L, x[18] - omega * (x[18] - e[18]));
+                REAL om = omega;
+                if (les) {
+                    /* SRC/col_MC.F90:302-306 */
+                    const REAL Ptotal = SQRT(FN(ptotal)(x, e));
+                    const REAL Ts = tauh + SQRT(cs18 * Ptotal + tau2) / (REAL)2;
+                    om = (REAL)1 / Ts;
+                }
+                for (int q = 0; q < 18; ++q) L->b[q][g] = ENC(L, x[q] - om * (x[q] - e[q]));
+                L->a[18][g] = ENC(L, x[18] - om * (x[18] - e[18]));
 #endif
             }
     for (int q = 0; q < 18; ++q) {
@@ -401,8 +477,13 @@ void FN(orc_step)(LAT *L, double svisc) {
 /* The same step written for a CPU: per row, 19 source-row pointers into the
    ghosted arrays and a vectorisable loop over i (each lane performs exactly
    the operations of FN(equilibrium) and the relaxation, so the result is
-   bit-identical to orc_step). Used as the timed CPU baseline. */
+   bit-identical to orc_step). Used as the timed CPU baseline. BGK collision
+   only: with the LES collision selected it runs orc_step. */
 void FN(orc_step_rows)(LAT *L, double svisc) {
+    if (L->les_cs > 0.0) {
+        FN(orc_step)(L, svisc);
+        return;
+    }
     FN(orc_boundaries)(L);
     const REAL omega = (REAL)FN(orc_omega)(svisc);
     const long l = L->l, m = L->m, n = L->n;

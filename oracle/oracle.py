@@ -53,6 +53,7 @@ def lib():
             f("orc_create").argtypes = [i, i, i]
             f("orc_destroy").argtypes = [vp]
             f("orc_set_scale").argtypes = [vp, d]
+            f("orc_set_les").argtypes = [vp, d]
             f("orc_init_tgv").argtypes = [vp, d, i]
             f("orc_init_velocity").argtypes = [vp, dp, dp, dp, d]
             f("orc_boundaries").argtypes = [vp]
@@ -123,6 +124,10 @@ class OracleLattice:
     def ncell(self):
         nx, ny, nz = self.shape
         return nx * ny * nz
+
+    def set_les(self, cs: float):
+        """LES collision of SRC/col_MC.F90:221-309 with cteS = cs (0: BGK)."""
+        self._f("orc_set_les")(self.h, cs)
 
     def init_tgv(self, u0: float, faithful: bool = True):
         self._f("orc_init_tgv")(self.h, u0, int(faithful))

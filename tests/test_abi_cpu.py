@@ -72,6 +72,7 @@ def test_defaults(bgk):
     dict(svisc=0.0), dict(svisc=-1.0), dict(svisc=float("nan")), dict(use_omega=1, omega=2.5),
     dict(fp16_scale=3.0), dict(fp16_scale=-2.0), dict(u0=float("inf")), dict(lx=4096, ly=4096, lz=4096),
     dict(kernel=3), dict(kernel=-1), dict(kernel=16),
+    dict(les_cs=-0.1), dict(les_cs=float("nan")), dict(les_cs=11.0),
 ])
 def test_create_rejects_bad_parameters_before_touching_a_device(bgk, bad):
     lib = bgk.load()

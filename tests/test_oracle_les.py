@@ -1,0 +1,139 @@
+"""CPU tests of the oracle's LES (Smagorinsky) collision, the block the
+reference compiles under -DLES (SRC/col_MC.F90:221-309): a single cell
+against the textbook Smagorinsky-BGK update in exact rational arithmetic
+(square roots in FP64), conservation, the BGK limit cs = 0, and the FP16
+form's restatement against the FP64 form."""
+from fractions import Fraction as Fr
+import math
+
+import numpy as np
+import pytest
+
+from test_oracle import CX, CY, CZ, W
+
+
+def _exact_les(x, omega, cs):
+    """f' = f - (f - f_eq)/tau_eff with Pi_ab = sum_q c_a c_b (f_q - f_eq_q),
+    |Pi| = sqrt(Pi:Pi), tau_eff = tau/2 + sqrt(18 cs^2 |Pi| + tau^2)/2,
+    tau = 1/omega. Rational arithmetic except for the two square roots."""
+    f = [Fr(v) + W[q] for q, v in enumerate(x)]
+    rho = sum(f)
+    u = [sum(f[q] * c[q] for q in range(19)) / rho for c in (CX, CY, CZ)]
+    usq = sum(a * a for a in u)
+    feq = []
+    for q in range(19):
+        cu = CX[q] * u[0] + CY[q] * u[1] + CZ[q] * u[2]
+        feq.append(W[q] * rho * (1 + 3 * cu + Fr(9, 2) * cu * cu - Fr(3, 2) * usq))
+    c = (CX, CY, CZ)
+    pi2 = Fr(0)
+    for a in range(3):
+        for b in range(3):
+            p = sum(c[a][q] * c[b][q] * (f[q] - feq[q]) for q in range(19))
+            pi2 += p * p
+    tau = 1 / Fr(omega)
+    ptot = math.sqrt(float(pi2))
+    teff = float(tau) / 2 + math.sqrt(18 * cs * cs * ptot + float(tau) ** 2) / 2
+    return [float(f[q] - W[q]) - (float(f[q] - feq[q])) / teff for q in range(19)]
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2])
+@pytest.mark.parametrize("cs", [0.1, 0.17, 0.5])
+def test_single_cell_les_matches_textbook_smagorinsky(oracle_mod, seed, cs):
+    O = oracle_mod
+    rng = np.random.default_rng(seed)
+    x = rng.uniform(-0.01, 0.01, 19)
+    L = O.OracleLattice(1, 1, 1)
+    L.set_les(cs)
+    L.put_pops(x.reshape(19, 1, 1, 1))
+    om = O.omega(1e-4)
+    L.col_mc_omega(om, periodic=True)
+    got = L.get_pops().reshape(19)
+    ref = _exact_les(x, om, cs)
+    for q in range(19):
+        assert abs(got[q] - ref[q]) <= 1e-15 + 1e-13 * abs(ref[q])
+    # the closure changed the update: it differs from plain BGK
+    B = O.OracleLattice(1, 1, 1)
+    B.put_pops(x.reshape(19, 1, 1, 1))
+    B.col_mc_omega(om, periodic=True)
+    assert not np.array_equal(B.get_pops(), L.get_pops())
+
+
+def test_les_zero_constant_is_bgk(oracle_mod):
+    O = oracle_mod
+    a, b = O.OracleLattice(6, 5, 4), O.OracleLattice(6, 5, 4)
+    for L in (a, b):
+        L.init_tgv(0.05)
+    a.set_les(0.0)
+    for _ in range(3):
+        a.step(0.01)
+        b.step(0.01)
+    assert np.array_equal(a.get_pops(), b.get_pops())
+
+
+@pytest.mark.parametrize("form", ["f64", "f32"])
+def test_les_conserves_mass_and_momentum(oracle_mod, form):
+    O = oracle_mod
+    L = O.OracleLattice(8, 9, 10, form=form)
+    L.init_tgv(0.05, faithful=False)
+    L.set_les(0.3)
+    d0 = L.get_dev()
+    for _ in range(20):
+        L.step(0.001)
+    d1 = L.get_dev()
+    # FP32: 720 cells x 20 steps of single-precision rounding near omega = 2
+    tol = 1e-13 if form == "f64" else 1e-4
+    assert abs(d1.sum() - d0.sum()) < tol
+    for c in (CX, CY, CZ):
+        m0 = np.tensordot(np.array(c, float), d0, axes=1).sum()
+        m1 = np.tensordot(np.array(c, float), d1, axes=1).sum()
+        assert abs(m1 - m0) < tol
+
+
+def test_les_fp16_form_tracks_fp64(oracle_mod):
+    """The FP16 form's LES restatement (its own moments and fused products)
+    follows the FP64 form as closely as the FP16 BGK form follows FP64 BGK
+    (binary16 storage error), while the closure visibly changes the result."""
+    O = oracle_mod
+    from bgk3d_hit_b200.hit import hit_velocity
+
+    n, scale = 12, 2.0 ** 16
+    u = hit_velocity(n, 2, 0.05, 7)
+    gap, res = {}, {}
+    for cs in (0.0, 0.17):
+        a = O.OracleLattice(n, n, n, "f64")
+        h = O.OracleLattice(n, n, n, "f16", scale=scale)
+        for L in (a, h):
+            L.init_velocity(*u)
+            L.set_les(cs)
+        for _ in range(10):
+            a.step(1e-4, periodic=True)
+            h.step(1e-4, periodic=True)
+        gap[cs] = np.max(np.abs(a.get_dev() - h.get_dev()))
+        res[cs] = a.get_dev()
+    assert gap[0.17] <= 1.5 * gap[0.0]
+    assert np.max(np.abs(res[0.17] - res[0.0])) > 5 * gap[0.0]
+
+
+def test_les_stabilises_an_under_resolved_box(oracle_mod):
+    """HIT at tau = 0.5002 (nu = 6.7e-5) on 24^3: BGK leaves the physical range
+    (|u| > 1 or non-finite) within 400 steps; the Smagorinsky closure with
+    cteS = 0.17 keeps it finite and decaying."""
+    O = oracle_mod
+    from bgk3d_hit_b200.hit import hit_velocity
+
+    n = 24
+    u = hit_velocity(n, 4, 0.08, 1234)
+    sv = 0.0002 / 3
+    out = {}
+    for cs in (0.0, 0.17):
+        L = O.OracleLattice(n, n, n, "f64")
+        L.init_velocity(*u)
+        L.set_les(cs)
+        for _ in range(400):
+            L.step(sv, periodic=True)
+        d = L.get_dev()
+        with np.errstate(all="ignore"):
+            ux = np.tensordot(np.array(CX, float), d, 1) / (d.sum(0) + 1.0)
+            out[cs] = float(np.sqrt(np.mean(ux * ux)))
+    assert not (out[0.0] < 1.0)  # blown up (or NaN)
+    assert np.isfinite(out[0.17]) and out[0.17] < 0.05

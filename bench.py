@@ -25,6 +25,14 @@ boundaries + col_MC). Prints one JSON line.
 Under torchrun, each rank runs an independent replica box on its own GPU
 (the path needs no collective on one box per GPU); value is the sum of the
 ranks' cell updates over the slowest rank's time.
+--decomp slabs: one box split along z instead (bgk3d_hit_b200.slabs): under
+torchrun each rank holds one size^3 slab of a size x size x (N size) box
+(weak scaling), the face populations go straight into the neighbours' ghost
+planes over NVLink (CUDA IPC) and a one-element NCCL all-reduce on the
+slab's stream separates the steps; on one GPU, --local-slabs P splits the
+size^3 box into P slabs in one process (the exchange and its host barrier
+measured without a second GPU). The HIT field of each rank's slab is the
+same size^3 tile.
 """
 from __future__ import annotations
 
@@ -62,6 +70,9 @@ def parse():
                     help="stream-collide kernel (0 automatic; 2/4 cells per thread apply to FP16; 8 TMA row pipeline)")
     ap.add_argument("--les-cs", type=float, default=0.0,
                     help="Smagorinsky constant: > 0 times the LES collision instead of BGK")
+    ap.add_argument("--decomp", default="replicas", choices=["replicas", "slabs"],
+                    help="N > 1: independent replica boxes (default) or one box split into z-slabs")
+    ap.add_argument("--local-slabs", type=int, default=2, help="--decomp slabs on one GPU: slabs per box")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
@@ -327,10 +338,92 @@ def run_ours(a):
         torch.distributed.destroy_process_group()
 
 
+def run_slabs(a):
+    """The z-slab decomposition: value = all slabs' cell updates / the slowest
+    slab's device time for K steps (each step: the slab kernels, then the
+    barrier)."""
+    import torch
+
+    from bgk3d_hit_b200.hit import hit_velocity
+    from bgk3d_hit_b200.slabs import DistSlabs, LocalSlabs, fp16_scale_for_velocity
+
+    rank, local, ws = dist_env()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+    if a.scheme != "two_lattice":
+        raise SystemExit("--decomp slabs runs the two-lattice scheme")
+    L = a.size
+    svisc = (a.tau - 0.5) / 3.0
+    u, v, w = hit_velocity(L, a.k0, 0.03, 1234)
+    kw = dict(svisc=svisc, u0=0.03, precision=a.precision, icheck=a.icheck, les_cs=a.les_cs)
+    if a.precision == "fp16":
+        kw["fp16_scale"] = fp16_scale_for_velocity(u, v, w)
+    if ws > 1:
+        drv = DistSlabs(L, L, L * ws, device=local, **kw)
+        boxes, nslab, cells = [drv.box], ws, float(L) ** 3 * ws
+    else:
+        drv = LocalSlabs(L, L, L, a.local_slabs, devices=(local,), **kw)
+        boxes, nslab, cells = drv.slabs, a.local_slabs, float(L) ** 3
+    drv.init_velocity(u, v, w)
+    streams = [torch.cuda.ExternalStream(b.stream, device=local) for b in boxes]
+    drv.run(a.warmup)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    l0 = sum(b.launch_count for b in boxes)
+    e0 = [torch.cuda.Event(enable_timing=True) for _ in boxes]
+    e1 = [torch.cuda.Event(enable_timing=True) for _ in boxes]
+    drv.barrier()
+    for e, s in zip(e0, streams):
+        e.record(s)
+    drv.run(a.steps)
+    for e, s in zip(e1, streams):
+        e.record(s)
+    torch.cuda.synchronize()
+    ms = max(e0[0].elapsed_time(e) for e in e1)
+    if ws > 1:
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    launches = sum(b.launch_count for b in boxes) - l0
+    clk = clocks.stop()
+    value = cells * a.steps / (ms * 1e-3) / 1e9
+    bpc = BYTES_PER_CELL[a.precision]
+    peak, peak_kind = measured_hbm()
+    achieved = bpc * (cells / ws) / (ms * 1e-3 / a.steps) / 1e9
+    if rank == 0:
+        line = {
+            "metric": "GLUPS (fused D3Q19 stream-collide)", "value": value, "unit": "GLUPS", "n_gpus": ws,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms / a.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": DTYPE[a.precision], "data": "synthetic",
+            "config": {"workload": workload_name(a) + f", split into {nslab} z-slabs",
+                       "box": [L, L, L * ws if ws > 1 else L], "precision": a.precision, "scheme": a.scheme,
+                       "tau": a.tau, "slabs": nslab, "gpus": ws,
+                       "l2": "inputs larger than L2" if cells * bpc / ws > 126e6 else "inputs may fit in L2",
+                       "parallelism": f"z-slabs, {'one per GPU' if ws > 1 else 'all on one GPU'}, ghost planes "
+                                      "filled by the step kernel (peer stores), barrier between steps"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind, "bytes_per_cell": bpc,
+                         "kernel": f"k_slab_{a.precision}", "per": "whole step of this GPU's slabs"},
+            "cpu_baseline": None, "e2e": None, "gpu_launches": launches, "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    drv.close()
+    if ws > 1:
+        torch.distributed.destroy_process_group()
+
+
 def main():
     a = parse()
     if a.impl == "reference":
         run_reference(a)
+    elif a.decomp == "slabs":
+        run_slabs(a)
     else:
         run_ours(a)
 

@@ -36,7 +36,7 @@ class BgkParams(C.Structure):
         ("precision", C.c_int), ("scheme", C.c_int), ("icheck", C.c_int), ("mode", C.c_int),
         ("fp16_scale", C.c_double), ("device", C.c_int),
         ("use_omega", C.c_int), ("omega", C.c_double), ("extras", C.c_int), ("kernel", C.c_int),
-        ("les_cs", C.c_double),
+        ("les_cs", C.c_double), ("proc_z", C.c_int), ("coord_z", C.c_int),
     ]
 
 
@@ -85,6 +85,11 @@ PROTOTYPES = [
     ("bgk_get_launch_count", _i, [_vp, C.POINTER(_ll)]),
     ("bgk_get_stream", _vp, [_vp]),
     ("bgk_synchronize", _i, [_vp]),
+    ("bgk_halo_buffer", _i, [_vp, C.POINTER(_vp), C.POINTER(C.c_size_t)]),
+    ("bgk_halo_ipc_handle", _i, [_vp, _vp]),
+    ("bgk_halo_ipc_open", _i, [_vp, _vp, C.POINTER(_vp)]),
+    ("bgk_halo_connect", _i, [_vp, _vp, _vp]),
+    ("bgk_halo_prime", _i, [_vp]),
     ("bgk_shift3", _i, [_vp, _vp, _vp, _vp, _vp, _vp, _i, _i, _i, _i, _i, _vp]),
     ("bgk_diagnostics_noalloc", _i, [C.POINTER(_vp), _i, _i, _i, _i, _i, _d, _d, _d, _d, _i, _i,
                                      C.POINTER(BgkDiag), _vp]),

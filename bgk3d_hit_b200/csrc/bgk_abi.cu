@@ -83,11 +83,42 @@ struct bgk_ctx {
   double* adj_acc = nullptr;
   long long adj_acc_n = 0;
   double* adj_tot = nullptr;
+  // z-slab (proc_z > 1): ghost buffer [parity 2][face 2][NZF][plane_elems],
+  // the neighbours' buffers, and whether the neighbours' planes were filled
+  // from the current state
+  int slab = 0;
+  void* halo_mem = nullptr;
+  size_t halo_bytes = 0;
+  long long plane_elems = 0;
+  void* nb_below = nullptr;
+  void* nb_above = nullptr;
+  int primed = 0;
+  std::vector<void*> ipc_maps;
 };
 
 namespace {
 
 long long ncell(const bgk_ctx* c) { return (long long)c->g.nx * c->g.ny * c->g.nz; }
+// cells of the whole box (all slabs)
+double global_cells(const bgk_ctx* c) { return (double)c->g.nx * (double)c->g.ny * (double)c->g.gz; }
+
+// Ghost-plane pointers of a slab: its own planes of parity rp (read) and the
+// neighbours' planes of parity wp (written); face 0 is the plane below a
+// slab (cz = +1 populations), face 1 the plane above (cz = -1).
+SlabLinks slab_links(const bgk_ctx* c, int rp, int wp) {
+  SlabLinks l{};
+  auto plane = [&](void* base, int par, int face, int s) -> void* {
+    if (!base) return nullptr;
+    return (char*)base + (size_t)(((par * 2 + face) * NZF + s) * c->plane_elems) * c->es;
+  };
+  for (int s = 0; s < NZF; ++s) {
+    l.in_lo[s] = plane(c->halo_mem, rp, 0, s);
+    l.in_hi[s] = plane(c->halo_mem, rp, 1, s);
+    l.up[s] = plane(c->nb_above, wp, 0, s);
+    l.dn[s] = plane(c->nb_below, wp, 1, s);
+  }
+  return l;
+}
 size_t rsize(const bgk_ctx* c) { return c->form == FORM_F64 ? 8 : 4; }
 
 int dev_alloc(bgk_ctx* c, void** ptr, size_t bytes, const char* what) {
@@ -190,12 +221,14 @@ int sync_and_check(bgk_ctx* c) {
 }
 
 int compute_diag(bgk_ctx* c, int itime, bgk_diag* out, int want_extras) {
-  const bool extras = want_extras && c->p.extras;
+  const bool extras = want_extras && c->p.extras && !c->slab;
   if (extras) {
     int rc = ensure_vel(c);
     if (rc) return rc;
   }
-  CK(launch_diag(c->A, c->lay, c->p.svisc, c->omega, c->scale, c->partials, extras ? c->vel : nullptr, c->st));
+  const SlabLinks hl = c->slab ? slab_links(c, (int)(c->step & 1), 0) : SlabLinks{};
+  CK(launch_diag(c->A, c->lay, c->p.svisc, c->omega, c->scale, c->partials, extras ? c->vel : nullptr, c->st,
+                 c->slab ? &hl : nullptr));
   c->launches++;
   if (extras) {
     CK(launch_enstrophy(c->A, c->vel, c->partials, c->st));
@@ -212,7 +245,8 @@ int compute_diag(bgk_ctx* c, int itime, bgk_diag* out, int want_extras) {
   int rc = sync_and_check(c);
   if (rc) return rc;
   const double* t = c->h_tot;
-  const double N = (double)ncell(c);
+  // a z-slab returns its contribution to the global means
+  const double N = global_cells(c);
   out->itime = itime;
   out->rho_mean = t[0] / N;
   out->ux_mean = t[1] / N;
@@ -236,7 +270,7 @@ int compute_diag(bgk_ctx* c, int itime, bgk_diag* out, int want_extras) {
     u0r = (double)(float)c->p.u0;
   }
   out->tke = t[5];
-  out->tke_norm = t[5] / (double)c->g.nx / (double)c->g.ny / (double)c->g.nz / (u0r * u0r);
+  out->tke_norm = t[5] / (double)c->g.nx / (double)c->g.ny / (double)c->g.gz / (u0r * u0r);
   out->diss = t[6];
   out->eps_strain = t[7] / N;
   out->nonfinite = (long long)t[8];
@@ -271,6 +305,8 @@ int bgk_params_default(bgk_params* p) {
   p->extras = 1;
   p->kernel = 0;
   p->les_cs = 0.0;
+  p->proc_z = 1;
+  p->coord_z = 0;
   return BGK_OK;
 }
 
@@ -282,10 +318,15 @@ int bgk_create(const bgk_params* p, bgk_ctx** out) {
   *out = nullptr;
   // parameter checks (the reference stops on inconsistent sizes,
   // SRC/input.F90:66-82; here every check returns an error instead)
-  if (p->lx < 1 || p->ly < 1 || p->lz < 1 || p->lz > 65535) {
-    set_err("invalid box %d x %d x %d", p->lx, p->ly, p->lz);
+  if (p->proc_z < 1 || p->coord_z < 0 || p->coord_z >= p->proc_z) {
+    set_err("invalid z decomposition: proc_z %d, coord_z %d", p->proc_z, p->coord_z);
     return BGK_ERR_INVALID;
   }
+  if (p->lx < 1 || p->ly < 1 || p->lz < 1 || p->lz % p->proc_z != 0 || p->lz / p->proc_z > 65535) {
+    set_err("invalid box %d x %d x %d for %d z-slab(s)", p->lx, p->ly, p->lz, p->proc_z);
+    return BGK_ERR_INVALID;
+  }
+  const int nzl = p->lz / p->proc_z;  // planes of this context
   if (p->precision < BGK_FP64 || p->precision > BGK_FP16DEV) {
     set_err("invalid precision %d", p->precision);
     return BGK_ERR_INVALID;
@@ -296,6 +337,11 @@ int bgk_create(const bgk_params* p, bgk_ctx** out) {
   }
   if (p->mode != BGK_CORRECTED && p->mode != BGK_FAITHFUL) {
     set_err("invalid mode %d", p->mode);
+    return BGK_ERR_INVALID;
+  }
+  if (p->proc_z > 1 && (p->scheme != BGK_TWO_LATTICE || p->mode != BGK_CORRECTED ||
+                        (p->precision == BGK_FP16DEV && p->fp16_scale == 0.0))) {
+    set_err("z-slabs run the two-lattice scheme in corrected mode, FP16 with an explicit fp16_scale");
     return BGK_ERR_INVALID;
   }
   if (p->kernel != 0 && p->kernel != 1 && p->kernel != 2 && p->kernel != 4 && p->kernel != 8) {
@@ -332,7 +378,7 @@ int bgk_create(const bgk_params* p, bgk_ctx** out) {
     }
   }
   const long long sx = ((long long)p->lx + ROW_ALIGN - 1) / ROW_ALIGN * ROW_ALIGN;
-  const long long cells = sx * p->ly * p->lz;
+  const long long cells = sx * p->ly * nzl;
   if (cells >= (1LL << 31) - POP_ALIGN) {
     set_err("box too large: %lld padded cells per population (limit 2^31)", cells);
     return BGK_ERR_INVALID;
@@ -356,9 +402,12 @@ int bgk_create(const bgk_params* p, bgk_ctx** out) {
   c->es = c->form == FORM_F64 ? 8 : (c->form == FORM_F32 ? 4 : 2);
   c->g.nx = p->lx;
   c->g.ny = p->ly;
-  c->g.nz = p->lz;
+  c->g.nz = nzl;
   c->g.sx = (int)sx;
   c->g.qs = (cells + POP_ALIGN - 1) / POP_ALIGN * POP_ALIGN;
+  c->g.z0 = p->coord_z * nzl;
+  c->g.gz = p->lz;
+  c->slab = p->proc_z > 1;
   c->omega = omega_of(*p, c->form);
   c->scale = c->form == FORM_F16 ? (p->fp16_scale != 0.0 ? p->fp16_scale : 1.0) : 1.0;
   c->A.form = c->B.form = c->form;
@@ -397,6 +446,14 @@ int bgk_create(const bgk_params* p, bgk_ctx** out) {
   c->A.err = c->B.err = c->d_err;
   e = cudaMallocHost((void**)&c->h_tot, (ND + 1) * sizeof(double));
   if (e != cudaSuccess) return fail(cuda_fail(e, "cudaMallocHost"));
+  if (c->slab) {
+    c->plane_elems = (sx * p->ly + POP_ALIGN - 1) / POP_ALIGN * POP_ALIGN;
+    c->halo_bytes = (size_t)(2 * 2 * NZF) * (size_t)c->plane_elems * c->es;
+    rc = dev_alloc(c, &c->halo_mem, c->halo_bytes, "ghost planes");
+    if (rc) return fail(rc);
+    e = cudaMemsetAsync(c->halo_mem, 0, c->halo_bytes, c->st);
+    if (e != cudaSuccess) return fail(cuda_fail(e, "cudaMemset"));
+  }
   c->lay = init_layout(c);
   *out = c;
   return BGK_OK;
@@ -419,6 +476,8 @@ int bgk_destroy(bgk_ctx* c) {
   cudaFree(c->fft_buf);
   cudaFree(c->d_bins);
   for (void* m : c->lat_pool) cudaFree(m);
+  for (void* m : c->ipc_maps) cudaIpcCloseMemHandle(m);
+  cudaFree(c->halo_mem);
   for (double* m : c->vel_pool) cudaFree(m);
   cudaFree(c->adj_acc);
   cudaFree(c->adj_tot);
@@ -447,6 +506,7 @@ int bgk_init_tgv(bgk_ctx* c) {
   c->lay = lay;
   c->step = 0;
   c->initialized = 1;
+  c->primed = 0;
   return BGK_OK;
 }
 
@@ -496,6 +556,7 @@ int bgk_init_velocity(bgk_ctx* c, const double* u, const double* v, const double
   c->lay = lay;
   c->step = 0;
   c->initialized = 1;
+  c->primed = 0;
   return BGK_OK;
 }
 
@@ -509,8 +570,17 @@ int bgk_col_mc(bgk_ctx* c, int itime) {
   int rc = check_init(c);
   if (rc) return rc;
   CK(cudaSetDevice(c->p.device));
-  if (c->scheme == BGK_TWO_LATTICE) {
+  if (c->slab && (!c->nb_below || !c->nb_above || !c->primed)) {
+    set_err("z-slab: call bgk_halo_connect and then bgk_halo_prime (after every new state) before stepping");
+    return BGK_ERR_STATE;
+  }
+  if (c->slab) {
+    const SlabLinks l = slab_links(c, (int)(c->step & 1), (int)((c->step + 1) & 1));
+    CK(launch_slab(c->A, c->B, l, c->omega, c->scale, c->p.les_cs, c->st));
+  } else if (c->scheme == BGK_TWO_LATTICE) {
     CK(launch_two_lattice(c->A, c->B, c->omega, c->scale, c->p.les_cs, c->p.kernel, c->st));
+  }
+  if (c->scheme == BGK_TWO_LATTICE) {
     // pointer swap of pops 01..18, SRC/col_MC.F90:364-421
     for (int q = 0; q < Q - 1; ++q) {
       void* t = c->A.p[q];
@@ -528,10 +598,102 @@ int bgk_col_mc(bgk_ctx* c, int itime) {
   return BGK_OK;
 }
 
+int bgk_halo_buffer(const bgk_ctx* c, void** dptr, size_t* bytes) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!dptr || !bytes || !c->slab) {
+    set_err("bgk_halo_buffer: null argument or not a z-slab context (proc_z = 1)");
+    return BGK_ERR_INVALID;
+  }
+  *dptr = c->halo_mem;
+  *bytes = c->halo_bytes;
+  return BGK_OK;
+}
+
+int bgk_halo_ipc_handle(const bgk_ctx* c, void* handle64) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!handle64 || !c->slab) {
+    set_err("bgk_halo_ipc_handle: null argument or not a z-slab context");
+    return BGK_ERR_INVALID;
+  }
+  static_assert(sizeof(cudaIpcMemHandle_t) == 64, "IPC handle size");
+  CK(cudaSetDevice(c->p.device));
+  cudaIpcMemHandle_t h;
+  CK(cudaIpcGetMemHandle(&h, c->halo_mem));
+  std::memcpy(handle64, &h, 64);
+  return BGK_OK;
+}
+
+int bgk_halo_ipc_open(bgk_ctx* c, const void* handle64, void** dptr) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!handle64 || !dptr || !c->slab) {
+    set_err("bgk_halo_ipc_open: null argument or not a z-slab context");
+    return BGK_ERR_INVALID;
+  }
+  CK(cudaSetDevice(c->p.device));
+  cudaIpcMemHandle_t h;
+  std::memcpy(&h, handle64, 64);
+  void* p = nullptr;
+  CK(cudaIpcOpenMemHandle(&p, h, cudaIpcMemLazyEnablePeerAccess));
+  c->ipc_maps.push_back(p);
+  *dptr = p;
+  return BGK_OK;
+}
+
+int bgk_halo_connect(bgk_ctx* c, void* below, void* above) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!below || !above || !c->slab) {
+    set_err("bgk_halo_connect: null buffer or not a z-slab context");
+    return BGK_ERR_INVALID;
+  }
+  CK(cudaSetDevice(c->p.device));
+  for (void* p : {below, above}) {
+    cudaPointerAttributes a{};
+    CK(cudaPointerGetAttributes(&a, p));
+    if (a.type != cudaMemoryTypeDevice) {
+      set_err("bgk_halo_connect: %p is not device memory", p);
+      return BGK_ERR_INVALID;
+    }
+    if (a.device != c->p.device) {
+      int ok = 0;
+      CK(cudaDeviceCanAccessPeer(&ok, c->p.device, a.device));
+      if (!ok) {
+        set_err("bgk_halo_connect: device %d cannot access device %d", c->p.device, a.device);
+        return BGK_ERR_INVALID;
+      }
+      cudaError_t e = cudaDeviceEnablePeerAccess(a.device, 0);
+      if (e == cudaErrorPeerAccessAlreadyEnabled) (void)cudaGetLastError();
+      else if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceEnablePeerAccess");
+    }
+  }
+  c->nb_below = below;
+  c->nb_above = above;
+  c->primed = 0;
+  return BGK_OK;
+}
+
+int bgk_halo_prime(bgk_ctx* c) {
+  int rc = check_init(c);
+  if (rc) return rc;
+  if (!c->slab || !c->nb_below || !c->nb_above) {
+    set_err("bgk_halo_prime: not a connected z-slab context");
+    return BGK_ERR_STATE;
+  }
+  CK(cudaSetDevice(c->p.device));
+  const SlabLinks l = slab_links(c, 0, (int)(c->step & 1));
+  CK(launch_halo_prime(c->A, l, c->st));
+  c->launches++;
+  c->primed = 1;
+  return BGK_OK;
+}
+
 int bgk_debug_stall_next_step(bgk_ctx* c) {
   int rc = check_ctx(c);
   if (rc) return rc;
-  if (c->p.kernel != 8 || c->p.les_cs > 0.0) {
+  if (c->p.kernel != 8 || c->p.les_cs > 0.0 || c->slab) {
     set_err("bgk_debug_stall_next_step needs the row-pipelined kernel (params.kernel = 8, BGK collision)");
     return BGK_ERR_INVALID;
   }
@@ -542,6 +704,10 @@ int bgk_debug_stall_next_step(bgk_ctx* c) {
 int bgk_run(bgk_ctx* c, int nsteps) {
   if (nsteps < 0) {
     set_err("nsteps < 0");
+    return BGK_ERR_INVALID;
+  }
+  if (c && c->slab && nsteps > 1) {
+    set_err("z-slab: one step per call, with the slabs synchronised between steps");
     return BGK_ERR_INVALID;
   }
   for (int s = 0; s < nsteps; ++s) {
@@ -640,6 +806,7 @@ int bgk_put_populations(bgk_ctx* c, const void* host) {
   c->lay = lay;
   if (!c->initialized) c->step = 0;
   c->initialized = 1;
+  c->primed = 0;
   return BGK_OK;
 }
 
@@ -672,6 +839,10 @@ int bgk_get_velocity(bgk_ctx* c, double* u, double* v, double* w) {
 int bgk_spectrum(bgk_ctx* c, int nbins, double* ek) {
   int rc = check_init(c);
   if (rc) return rc;
+  if (c->slab) {
+    set_err("bgk_spectrum needs the whole box (proc_z = 1)");
+    return BGK_ERR_INVALID;
+  }
   if (!ek || nbins < 1) {
     set_err("bgk_spectrum: invalid argument");
     return BGK_ERR_INVALID;
@@ -830,6 +1001,7 @@ int bgk_load(bgk_ctx* c, const char* path) {
   c->step = h.step;
   if (c->form == FORM_F16) c->scale = h.scale;
   c->initialized = 1;
+  c->primed = 0;
   return BGK_OK;
 }
 
@@ -854,10 +1026,12 @@ int bgk_vtk(bgk_ctx* c, int itime, int kind, int index, const char* dir) {
   rc = sync_and_check(c);
   if (rc) return rc;
   // legacy VTK, as SRC/vtk_xy.binary.F90:58-97 writes it: ASCII header with
-  // I10 fields, then big-endian float32 velocity triples
+  // I10 fields, then big-endian float32 velocity triples; a z-slab writes its
+  // own file named by its rank, with its z offset in ORIGIN (offset(3),
+  // SRC/vtk_xy.binary.F90:53,65-67), and an xy index local to the slab
   static const char* tag[4] = {"3d", "xy", "xz", "yz"};
   char name[64];
-  snprintf(name, sizeof(name), "tec_%s.%05d.%08d.vtk", tag[kind], 0, itime);
+  snprintf(name, sizeof(name), "tec_%s.%05d.%08d.vtk", tag[kind], c->p.coord_z, itime);
   const std::string path = std::string(dir && *dir ? dir : ".") + "/" + name;
   FileCloser fc{fopen(path.c_str(), "wb")};
   if (!fc.f) {
@@ -865,7 +1039,8 @@ int bgk_vtk(bgk_ctx* c, int itime, int kind, int index, const char* dir) {
     return BGK_ERR_INVALID;
   }
   const int dims[4][3] = {{nx, ny, nz}, {nx, ny, 1}, {nx, 1, nz}, {1, ny, nz}};
-  const int orig[4][3] = {{1, 1, 1}, {1, 1, index}, {1, index, 1}, {index, 1, 1}};
+  const int z0 = c->g.z0;
+  const int orig[4][3] = {{1, 1, z0 + 1}, {1, 1, z0 + index}, {1, index, z0 + 1}, {index, 1, z0 + 1}};
   fprintf(fc.f, "# vtk DataFile Version 2.0\nCampo\nBINARY\nDATASET STRUCTURED_POINTS\n");
   fprintf(fc.f, "DIMENSIONS %10d %10d %10d\n", dims[kind][0], dims[kind][1], dims[kind][2]);
   fprintf(fc.f, "ORIGIN %10d %10d %10d\n", orig[kind][0], orig[kind][1], orig[kind][2]);
@@ -934,6 +1109,10 @@ int adj_check(bgk_ctx* c, int nsteps) {
   if (rc) return rc;
   if (c->form == FORM_F16) {
     set_err("the adjoint and tangent models support the FP64 and FP32 forms");
+    return BGK_ERR_INVALID;
+  }
+  if (c->slab) {
+    set_err("the adjoint and tangent models run on a whole box (proc_z = 1)");
     return BGK_ERR_INVALID;
   }
   if (c->p.les_cs > 0.0) {

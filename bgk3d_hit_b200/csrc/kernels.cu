@@ -282,6 +282,73 @@ __global__ void __launch_bounds__(256) k_aa(Pops<typename F::S> a, Geo g, StepK 
   }
 }
 
+// ----------------------------------------------------------------- z-slabs
+// Two-lattice step of one z-slab of a box split along z (the reference's
+// proc_z ranks, SRC/setup_MPI.F90:112-131). x and y wrap in the kernel; a pull
+// across a z face reads this slab's ghost plane instead of wrapping. The
+// boundary planes' post-collision populations that cross a face are also
+// stored straight into the neighbour's ghost plane for the next step (a peer
+// store over NVLink when the neighbour is another GPU): the halo exchange of
+// SRC/bcond.comm.step3.F90:77-297 fused into the producing kernel.
+template <class F, bool LES = false>
+__global__ void __launch_bounds__(256) k_slab(Pops<const typename F::S> src, Pops<typename F::S> dst, Geo g,
+                                              StepK K, Halo<typename F::S> h) {
+  using S = typename F::S;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  if (i >= g.nx || j >= g.ny) return;
+  const int im = i == 0 ? g.nx - 1 : i - 1, ip = i == g.nx - 1 ? 0 : i + 1;
+  const int jm = j == 0 ? g.ny - 1 : j - 1, jp = j == g.ny - 1 ? 0 : j + 1;
+  S v[Q];
+#pragma unroll
+  for (int q = 0; q < Q; ++q) {
+    const int ii = cxq(q) > 0 ? im : (cxq(q) < 0 ? ip : i);
+    const int jj = cyq(q) > 0 ? jm : (cyq(q) < 0 ? jp : j);
+    const int po = ii + g.sx * jj;
+    if (czq(q) > 0 && k == 0) v[q] = ldg(h.in_lo[zslot(q)] + po);
+    else if (czq(q) < 0 && k == g.nz - 1) v[q] = ldg(h.in_hi[zslot(q)] + po);
+    else {
+      const int off = po + g.sx * g.ny * (k - czq(q));
+      v[q] = (q == Q - 1) ? src.p[Q - 1][off] : ldg(src.p[q] + off);
+    }
+  }
+  F::template cell<LES>(v, K);
+  const int po = i + g.sx * j;
+  const int o = po + g.sx * g.ny * k;
+#pragma unroll
+  for (int q = 0; q < Q; ++q) dst.p[q][o] = v[q];
+  if (k == g.nz - 1) {
+#pragma unroll
+    for (int q = 0; q < Q; ++q)
+      if (czq(q) > 0) h.up[zslot(q)][po] = v[q];
+  }
+  if (k == 0) {
+#pragma unroll
+    for (int q = 0; q < Q; ++q)
+      if (czq(q) < 0) h.dn[zslot(q)][po] = v[q];
+  }
+  // peer stores are made visible system-wide before the thread ends
+  if (k == 0 || k == g.nz - 1) __threadfence_system();
+}
+
+// Fills the neighbours' ghost planes from this slab's current boundary planes
+// (after an initial condition, an upload or a restart).
+template <class S>
+__global__ void k_halo_prime(Pops<const S> a, Geo g, Halo<S> h) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y;
+  if (i >= g.nx) return;
+  const int po = i + g.sx * j;
+  const long long top = po + (long long)g.sx * g.ny * (g.nz - 1);
+#pragma unroll
+  for (int q = 0; q < Q; ++q) {
+    if (czq(q) > 0) h.up[zslot(q)][po] = a.p[q][top];
+    if (czq(q) < 0) h.dn[zslot(q)][po] = a.p[q][po];
+  }
+  __threadfence_system();
+}
+
 // ------------------------------------------------------ initial conditions
 // Per-cell equilibrium deviation of SRC/init.F90:97-137 (cte1 = 0):
 // out_q = crho*w_q*(0 + rf*(c.u) + qf*(3*(c.u)^2 - |u|^2)), with each linear
@@ -353,18 +420,20 @@ __global__ void k_init_tgv(Pops<typename F::S> a, Geo g, int lay, typename F::R 
   float tmax = 0.f;
   for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
     const int i = (int)(c % g.nx), j = (int)((c / g.nx) % g.ny), k = (int)(c / ((long long)g.nx * g.ny));
-    // reference interior indices are 1-based
-    const int ir = i + 1, jr = j + 1, kr = k + 1;
+    // reference interior indices are 1-based; a z-slab uses global z
+    // (k0 + k with k0 = offset(3), SRC/init.F90:73,84)
+    const int ir = i + 1, jr = j + 1, kr = g.z0 + k + 1;
+    const int gz = g.gz > 0 ? g.gz : g.nz;
     R x, y, z, pi;
     if (faithful) {
       x = (R)(((float)ir - 0.5f) / (float)g.nx);
       y = (R)(((float)jr - 0.5f) / (float)g.ny);
-      z = (R)(((float)kr - 0.5f) / (float)g.nz);
+      z = (R)(((float)kr - 0.5f) / (float)gz);
       pi = (R)3.141592653589793238462643383279f;
     } else {
       x = (R)(((double)ir - 0.5) / (double)g.nx);
       y = (R)(((double)jr - 0.5) / (double)g.ny);
-      z = (R)(((double)kr - 0.5) / (double)g.nz);
+      z = (R)(((double)kr - 0.5) / (double)gz);
       pi = (R)3.141592653589793238462643383279;
     }
     const V two = N::c(2.0), four = N::c(4.0), u0 = N::wrap(u0r), P = N::wrap(pi);
@@ -445,7 +514,7 @@ __global__ void k_import(Pops<typename F::S> a, Geo g, int q, const typename F::
 template <class F, int LAY>
 __global__ void __launch_bounds__(DIAG_THREADS) k_diag(Pops<const typename F::S> a, Geo g, double svisc,
                                                        double omega, typename F::R inv, double* partials,
-                                                       typename F::R* vel) {
+                                                       typename F::R* vel, Halo<typename F::S> h) {
   using R = typename F::R; using V = typename F::V; using N = Num<V>;
   __shared__ KS sh[DIAG_THREADS];
   KS acc[ND];
@@ -471,8 +540,16 @@ __global__ void __launch_bounds__(DIAG_THREADS) k_diag(Pops<const typename F::S>
       acc[8].s = __dadd_rn(acc[8].s, 1.0);
     if (vel) { vel[c] = N::raw(ux); vel[n + c] = N::raw(uy); vel[2 * n + c] = N::raw(uz); }
 #pragma unroll
-    for (int q = 0; q < Q; ++q)
-      x[q] = N::wrap(F::dec(a.p[ref_slot<LAY>(q)][ref_off<LAY>(g, q, i, j, k, -cxq(q), -cyq(q), -czq(q))], inv));
+    for (int q = 0; q < Q; ++q) {
+      // a z-slab pulls across its faces from its ghost planes
+      const bool lo = czq(q) > 0 && k == 0, hi = czq(q) < 0 && k == g.nz - 1;
+      if (LAY == LAY_TWO && h.in_lo[0] && (lo || hi)) {
+        const int po = wrapi(i - cxq(q), g.nx) + g.sx * wrapi(j - cyq(q), g.ny);
+        x[q] = N::wrap(F::dec(lo ? h.in_lo[zslot(q)][po] : h.in_hi[zslot(q)][po], inv));
+      } else {
+        x[q] = N::wrap(F::dec(a.p[ref_slot<LAY>(q)][ref_off<LAY>(g, q, i, j, k, -cxq(q), -cyq(q), -czq(q))], inv));
+      }
+    }
     V e[Q], vx, vy, vz;
     const V rp = equilibrium<V>(x, e, vx, vy, vz);
     const V vsq = vx * vx + vy * vy + vz * vz;
@@ -845,27 +922,79 @@ cudaError_t launch_import(const Lattice& a, int lay, int q, const void* ds, cuda
   return cudaErrorInvalidValue;
 }
 
+template <class S> static Halo<S> halo_of(const SlabLinks* l) {
+  Halo<S> h{};
+  if (!l) return h;
+  for (int s = 0; s < NZF; ++s) {
+    h.in_lo[s] = (const S*)l->in_lo[s];
+    h.in_hi[s] = (const S*)l->in_hi[s];
+    h.up[s] = (S*)l->up[s];
+    h.dn[s] = (S*)l->dn[s];
+  }
+  return h;
+}
+
 template <class F, int LAY>
 static void diag_lay(const Lattice& a, double svisc, double omega, double scale, double* partials, void* vel,
-                     cudaStream_t st) {
+                     const SlabLinks* halo, cudaStream_t st) {
   using S = typename F::S; using R = typename F::R;
   k_diag<F, LAY><<<DIAG_BLOCKS, DIAG_THREADS, 0, st>>>(pops_of<const S>(a), a.g, svisc, omega, (R)(1.0 / scale),
-                                                       partials, (R*)vel);
+                                                       partials, (R*)vel, halo_of<S>(halo));
 }
 template <class F>
 static cudaError_t diag_impl(const Lattice& a, int lay, double svisc, double omega, double scale, double* partials,
-                             void* vel, cudaStream_t st) {
-  if (lay == LAY_TWO) diag_lay<F, LAY_TWO>(a, svisc, omega, scale, partials, vel, st);
-  else if (lay == LAY_AAE) diag_lay<F, LAY_AAE>(a, svisc, omega, scale, partials, vel, st);
-  else diag_lay<F, LAY_AAN>(a, svisc, omega, scale, partials, vel, st);
+                             void* vel, const SlabLinks* halo, cudaStream_t st) {
+  if (lay == LAY_TWO) diag_lay<F, LAY_TWO>(a, svisc, omega, scale, partials, vel, halo, st);
+  else if (lay == LAY_AAE) diag_lay<F, LAY_AAE>(a, svisc, omega, scale, partials, vel, halo, st);
+  else diag_lay<F, LAY_AAN>(a, svisc, omega, scale, partials, vel, halo, st);
   return cudaGetLastError();
 }
 cudaError_t launch_diag(const Lattice& a, int lay, double svisc, double omega, double scale, double* partials,
-                        void* vel, cudaStream_t st) {
+                        void* vel, cudaStream_t st, const SlabLinks* halo) {
   switch (a.form) {
-    case FORM_F64: return diag_impl<F64>(a, lay, svisc, omega, scale, partials, vel, st);
-    case FORM_F32: return diag_impl<F32>(a, lay, svisc, omega, scale, partials, vel, st);
-    case FORM_F16: return diag_impl<F16>(a, lay, svisc, omega, scale, partials, vel, st);
+    case FORM_F64: return diag_impl<F64>(a, lay, svisc, omega, scale, partials, vel, halo, st);
+    case FORM_F32: return diag_impl<F32>(a, lay, svisc, omega, scale, partials, vel, halo, st);
+    case FORM_F16: return diag_impl<F16>(a, lay, svisc, omega, scale, partials, vel, halo, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+template <class F>
+static cudaError_t slab_impl(const Lattice& s, const Lattice& d, const StepK& K, const SlabLinks& l,
+                             cudaStream_t st) {
+  using S = typename F::S;
+  Pops<const S> ps = pops_of<const S>(s);
+  Pops<S> pd = pops_of<S>(d);
+  pd.p[Q - 1] = (S*)s.p[Q - 1];  // pop 19 in place (SRC/col_MC.F90:351)
+  const Shape sh = cell_shape(s.g);
+  if (K.les) k_slab<F, true><<<sh.grid, sh.block, 0, st>>>(ps, pd, s.g, K, halo_of<S>(&l));
+  else k_slab<F, false><<<sh.grid, sh.block, 0, st>>>(ps, pd, s.g, K, halo_of<S>(&l));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_slab(const Lattice& src, const Lattice& dst, const SlabLinks& links, double omega, double scale,
+                        double les_cs, cudaStream_t st) {
+  const StepK K = make_stepk(src.form, omega, scale, les_cs);
+  switch (src.form) {
+    case FORM_F64: return slab_impl<F64>(src, dst, K, links, st);
+    case FORM_F32: return slab_impl<F32>(src, dst, K, links, st);
+    case FORM_F16: return slab_impl<F16>(src, dst, K, links, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+template <class S>
+static cudaError_t prime_impl(const Lattice& a, const SlabLinks& l, cudaStream_t st) {
+  const int tx = a.g.nx >= 256 ? 256 : ((a.g.nx + 31) / 32) * 32;
+  k_halo_prime<S><<<dim3((a.g.nx + tx - 1) / tx, a.g.ny), tx, 0, st>>>(pops_of<const S>(a), a.g, halo_of<S>(&l));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_halo_prime(const Lattice& a, const SlabLinks& links, cudaStream_t st) {
+  switch (a.form) {
+    case FORM_F64: return prime_impl<double>(a, links, st);
+    case FORM_F32: return prime_impl<float>(a, links, st);
+    case FORM_F16: return prime_impl<__half>(a, links, st);
   }
   return cudaErrorInvalidValue;
 }

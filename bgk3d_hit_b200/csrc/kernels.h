@@ -21,6 +21,16 @@ struct Lattice {
   int stall = 0;       // test hook: the next pipelined launch waits on a barrier nothing arms
 };
 
+// Ghost-plane pointers of a z-slab for one step (see Halo in lattice.cuh):
+// in_lo / in_hi this slab's planes read this step, up / dn the neighbours'
+// planes written for the next step.
+struct SlabLinks {
+  void* in_lo[NZF];
+  void* in_hi[NZF];
+  void* up[NZF];
+  void* dn[NZF];
+};
+
 // Modes of the row-pipelined kernel (rows.cu).
 enum RowMode { ROW_TWO = 0, ROW_AA_EVEN = 1, ROW_AA_ODD = 2 };
 
@@ -87,8 +97,17 @@ cudaError_t launch_import(const Lattice& a, int lay, int q, const void* dense_st
 
 // Diagnostics: per-block partial sums (Neumaier pairs) of ND quantities.
 // vel (optional, 3*N values of the arithmetic type) receives the local velocity.
+// halo: the ghost planes of a z-slab (in_lo / in_hi), nullptr for a whole box.
 cudaError_t launch_diag(const Lattice& a, int lay, double svisc, double omega, double scale, double* partials,
-                        void* vel, cudaStream_t st);
+                        void* vel, cudaStream_t st, const SlabLinks* halo = nullptr);
+
+// z-slab two-lattice step (src -> dst, pop 19 in place) reading the ghost
+// planes links.in_* and storing the outgoing boundary populations into
+// links.up / links.dn; and the fill of links.up / links.dn from the current
+// state alone.
+cudaError_t launch_slab(const Lattice& src, const Lattice& dst, const SlabLinks& links, double omega, double scale,
+                        double les_cs, cudaStream_t st);
+cudaError_t launch_halo_prime(const Lattice& a, const SlabLinks& links, cudaStream_t st);
 cudaError_t launch_enstrophy(const Lattice& a, const void* vel, double* partials, cudaStream_t st);
 // Sums DIAG_BLOCKS partials into ND totals (fixed order, compensated).
 cudaError_t launch_finalize(const double* partials, double* totals, cudaStream_t st);

@@ -26,6 +26,14 @@ __host__ __device__ constexpr int czq(int q) {
   return (q == 1 || q == 8 || q == 10 || q == 14 || q == 15) ? -1
          : (q == 3 || q == 5 || q == 6 || q == 12 || q == 17) ? 1 : 0;
 }
+// Populations that cross a z face: cz = +1 (q = 3, 5, 6, 12, 17; reference
+// 4, 6, 7, 13, 18) and cz = -1 (q = 1, 8, 10, 14, 15; reference 2, 9, 11, 15,
+// 16), the five per face that SRC/bcond.comm.step3.F90:77-297 exchanges.
+// zslot(q) is the position of q in its list.
+constexpr int NZF = 5;
+__host__ __device__ constexpr int zslot(int q) {
+  return (q == 3 || q == 1) ? 0 : (q == 5 || q == 8) ? 1 : (q == 6 || q == 10) ? 2 : (q == 12 || q == 14) ? 3 : 4;
+}
 // Opposite direction, c(opp q) = -c(q). Pairs in the reference's 1-based
 // numbering: 1<->12, 2<->13, 3<->10, 4<->11, 5<->14, 6<->15, 7<->16, 8<->17,
 // 9<->18, 19 fixed.
@@ -273,6 +281,20 @@ struct Geo {
   int nx, ny, nz;
   int sx;          // row pitch, elements (multiple of 32)
   long long qs;    // population stride, elements
+  int z0 = 0;      // z-slab: global index of local plane 0 (0 for a whole box)
+  int gz = 0;      // z-slab: global box height (nz for a whole box)
+};
+
+// Ghost planes of a z-slab. The plane below the slab (z = -1) holds the five
+// cz = +1 populations, the plane above (z = nz) the five cz = -1 ones, each a
+// sx*ny plane indexed i + sx*j. `in` are this slab's ghost planes for the
+// current step; `up` / `dn` are the neighbours' planes (above: its lower plane;
+// below: its upper plane) that this step's boundary planes fill for the next.
+template <class S> struct Halo {
+  const S* in_lo[NZF];
+  const S* in_hi[NZF];
+  S* up[NZF];
+  S* dn[NZF];
 };
 
 template <class S> struct Pops { S* p[Q]; };

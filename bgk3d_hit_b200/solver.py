@@ -54,7 +54,7 @@ class BGK3D:
     def __init__(self, lx: int = 64, ly: int | None = None, lz: int | None = None, *, svisc: float = 0.01,
                  u0: float = 0.05, precision: str = "fp64", scheme: str = "two_lattice", icheck: int = 10,
                  mode: str = "corrected", fp16_scale: float = 0.0, device: int = 0, omega: float | None = None,
-                 extras: bool = True, kernel: int = 0, les_cs: float = 0.0):
+                 extras: bool = True, kernel: int = 0, les_cs: float = 0.0, proc_z: int = 1, coord_z: int = 0):
         self._lib = _abi.load()
         p = BgkParams()
         check(self._lib.bgk_params_default(C.byref(p)), "bgk_params_default")
@@ -64,13 +64,15 @@ class BGK3D:
         p.scheme = _abi.SCHEMES[scheme] if isinstance(scheme, str) else int(scheme)
         p.mode = _abi.MODES[mode] if isinstance(mode, str) else int(mode)
         p.icheck, p.fp16_scale, p.device, p.extras, p.kernel = icheck, fp16_scale, device, int(extras), kernel
-        p.les_cs = les_cs
+        p.les_cs, p.proc_z, p.coord_z = les_cs, proc_z, coord_z
         if omega is not None:
             p.use_omega, p.omega = 1, omega
         self.params = p
         self._h = C.c_void_p()
         check(self._lib.bgk_create(C.byref(p), C.byref(self._h)), "bgk_create")
-        self.shape = (p.lx, p.ly, p.lz)
+        # local shape: a z-slab (proc_z > 1) holds lz/proc_z planes
+        self.shape = (p.lx, p.ly, p.lz // max(proc_z, 1))
+        self.global_shape = (p.lx, p.ly, p.lz)
         self.dtype = _STORE_DTYPES[p.precision]
 
     # ----------------------------------------------------------- set-up
@@ -78,9 +80,10 @@ class BGK3D:
     def from_input(cls, path: str, **kw) -> "BGK3D":
         """input + hencol + alloca from a bgk.input namelist (one rank)."""
         nl = read_namelist(path)
-        for ax in ("x", "y", "z"):
+        for ax in ("x", "y"):
             if nl.get("proc_" + ax, 1) != 1:
-                raise ValueError("one box per GPU: proc_x = proc_y = proc_z = 1")
+                raise ValueError("the box is split along z only: proc_x = proc_y = 1")
+        kw.setdefault("proc_z", nl.get("proc_z", 1))
         return cls(nl["lx"], nl["ly"], nl["lz"], svisc=nl["svisc"], u0=nl["u0"], icheck=nl.get("icheck", 100), **kw)
 
     def close(self):
@@ -235,6 +238,31 @@ class BGK3D:
 
     def synchronize(self):
         check(self._lib.bgk_synchronize(self._h), "bgk_synchronize")
+
+    # ---------------------------------------------------------- z-slabs
+    # The halo exchange of SRC/bcond.comm.step3.F90 for a box split along z
+    # (proc_z > 1); the orchestration across slabs is in slabs.py.
+    def halo_buffer(self) -> tuple[int, int]:
+        ptr, n = C.c_void_p(), C.c_size_t()
+        check(self._lib.bgk_halo_buffer(self._h, C.byref(ptr), C.byref(n)), "bgk_halo_buffer")
+        return ptr.value, n.value
+
+    def halo_ipc_handle(self) -> bytes:
+        buf = C.create_string_buffer(64)
+        check(self._lib.bgk_halo_ipc_handle(self._h, buf), "bgk_halo_ipc_handle")
+        return buf.raw
+
+    def halo_ipc_open(self, handle: bytes) -> int:
+        ptr = C.c_void_p()
+        check(self._lib.bgk_halo_ipc_open(self._h, C.create_string_buffer(bytes(handle), 64), C.byref(ptr)),
+              "bgk_halo_ipc_open")
+        return ptr.value
+
+    def halo_connect(self, below: int, above: int):
+        check(self._lib.bgk_halo_connect(self._h, C.c_void_p(below), C.c_void_p(above)), "bgk_halo_connect")
+
+    def halo_prime(self):
+        check(self._lib.bgk_halo_prime(self._h), "bgk_halo_prime")
 
 
 def run_loop(box: BGK3D, itfin: int, out_dir: str | None = None, itstart: int = 1, ivtim: int | None = None,

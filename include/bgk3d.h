@@ -33,6 +33,8 @@
 #ifndef BGK3D_H
 #define BGK3D_H
 
+#include <stddef.h>
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -93,6 +95,15 @@ typedef struct {
                           0 (default) = plain BGK. The LES collision runs on the one
                           cell per thread kernels (kernel 2/4/8 fall back to them);
                           bgk_adjoint and bgk_tangent reject it. */
+  int proc_z;          /* number of z-slabs the box is split into (the reference's
+                          proc_z, SRC/input.F90:41; proc_x = proc_y = 1). 1 (default):
+                          one whole periodic box. > 1: this context holds slab
+                          coord_z, lz/proc_z planes starting at global plane
+                          coord_z*lz/proc_z (lz is the global height and must be a
+                          multiple of proc_z, as SRC/input.F90:66-82 requires); see
+                          "z-slabs" below. */
+  int coord_z;         /* this slab's index, 0..proc_z-1 (the rank's z coordinate in
+                          the reference's MPI_Cart topology, SRC/setup_MPI.F90:112-131) */
 } bgk_params;
 
 /* Diagnostics of one step, in FP64. */
@@ -229,6 +240,50 @@ int bgk_get_launch_count(const bgk_ctx* ctx, long long* count);
 void* bgk_get_stream(const bgk_ctx* ctx);
 /* Waits for all work of the context. */
 int bgk_synchronize(bgk_ctx* ctx);
+
+/* z-slabs (proc_z > 1): the halo exchange of bcond_comm_step3
+   (SRC/bcond.comm.step3.F90:77-297, five populations per z face) without
+   messages. Each slab owns a ghost buffer: two step parities x two faces x
+   five populations x one lx*ly plane (padded rows). The step kernel reads its
+   own ghost planes and stores its boundary planes' crossing populations
+   directly into the neighbours' ghost buffers for the next step - device
+   pointers that may live on another GPU (peer stores over NVLink / NVSwitch).
+   Contract for the caller (one process per GPU, or several slabs in one
+   process):
+     1. bgk_halo_buffer / bgk_halo_ipc_handle: publish each slab's buffer;
+     2. bgk_halo_connect(ctx, below, above): give each slab the buffers of
+        slabs coord_z-1 and coord_z+1 (mod proc_z) as device pointers usable
+        from its device (same process: the pointers themselves; another
+        process: bgk_halo_ipc_open);
+     3. after every initial condition, bgk_put_populations or bgk_load:
+        bgk_halo_prime on every slab;
+     4. between consecutive bgk_col_mc / bgk_halo_prime / diagnostic calls of
+        different slabs, every slab's previous call must have completed on the
+        device before any slab's next call starts (a barrier: a stream-ordered
+        collective such as a one-element NCCL all-reduce on the contexts'
+        streams, or bgk_synchronize on every slab plus a host barrier).
+   bgk_col_mc then advances one slab by one step (bgk_run accepts nsteps <= 1),
+   the diagnostics return this slab's contribution to the global means (sums
+   divided by the global cell count: the global value is the sum over the
+   slabs), and bgk_vtk writes the slab's file with its rank number and z
+   offset as the reference's per-rank writers do. z-slabs run the
+   two-lattice scheme in corrected mode; FP16 needs an explicit fp16_scale
+   (the same on every slab); enstrophy, bgk_spectrum, bgk_adjoint and
+   bgk_tangent are not available on a slab. */
+/* This slab's ghost buffer (device pointer and size in bytes). */
+int bgk_halo_buffer(const bgk_ctx* ctx, void** dptr, size_t* bytes);
+/* cudaIpcGetMemHandle of the ghost buffer into handle[64]. */
+int bgk_halo_ipc_handle(const bgk_ctx* ctx, void* handle64);
+/* Maps another process's ghost buffer (handle from bgk_halo_ipc_handle) into
+   this context's device; the mapping is released by bgk_destroy. */
+int bgk_halo_ipc_open(bgk_ctx* ctx, const void* handle64, void** dptr);
+/* Sets the ghost buffers of the slab below (coord_z - 1) and above
+   (coord_z + 1), periodic in coord_z; enables peer access when they are on
+   another device of this process. */
+int bgk_halo_connect(bgk_ctx* ctx, void* below, void* above);
+/* Stores this slab's boundary planes into the neighbours' ghost buffers for
+   the current step (after an initial condition, upload or restart). */
+int bgk_halo_prime(bgk_ctx* ctx);
 
 /* Streaming-only calibrator, the single-box equivalent of do_somethingGPU
    (SRC/do_somethingGPU.F90:37-100) without the MPI barrier: out1(i,j,k) =

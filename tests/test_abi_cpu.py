@@ -73,6 +73,8 @@ def test_defaults(bgk):
     dict(fp16_scale=3.0), dict(fp16_scale=-2.0), dict(u0=float("inf")), dict(lx=4096, ly=4096, lz=4096),
     dict(kernel=3), dict(kernel=-1), dict(kernel=16),
     dict(les_cs=-0.1), dict(les_cs=float("nan")), dict(les_cs=11.0),
+    dict(proc_z=0), dict(proc_z=2, coord_z=2), dict(proc_z=2, coord_z=-1), dict(proc_z=3),
+    dict(proc_z=2, scheme=1), dict(proc_z=2, mode=1), dict(proc_z=2, precision=2),
 ])
 def test_create_rejects_bad_parameters_before_touching_a_device(bgk, bad):
     lib = bgk.load()

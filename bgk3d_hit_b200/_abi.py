@@ -85,6 +85,8 @@ PROTOTYPES = [
     ("bgk_get_launch_count", _i, [_vp, C.POINTER(_ll)]),
     ("bgk_get_stream", _vp, [_vp]),
     ("bgk_synchronize", _i, [_vp]),
+    ("bgk_record_event", _i, [_vp]),
+    ("bgk_wait_event", _i, [_vp, _vp]),
     ("bgk_halo_buffer", _i, [_vp, C.POINTER(_vp), C.POINTER(C.c_size_t)]),
     ("bgk_halo_ipc_handle", _i, [_vp, _vp]),
     ("bgk_halo_ipc_open", _i, [_vp, _vp, C.POINTER(_vp)]),

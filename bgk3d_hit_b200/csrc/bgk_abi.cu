@@ -51,6 +51,7 @@ struct bgk_ctx {
   bgk_params p;
   int form = 0, scheme = 0;
   cudaStream_t st = nullptr;
+  cudaEvent_t mark = nullptr;  // bgk_record_event / bgk_wait_event
   Geo g{};
   size_t es = 8;
   void* memA = nullptr;
@@ -482,6 +483,7 @@ int bgk_destroy(bgk_ctx* c) {
   cudaFree(c->adj_acc);
   cudaFree(c->adj_tot);
   if (c->h_tot) cudaFreeHost(c->h_tot);
+  if (c->mark) cudaEventDestroy(c->mark);
   if (c->st) cudaStreamDestroy(c->st);
   delete c;
   return BGK_OK;
@@ -577,6 +579,7 @@ int bgk_col_mc(bgk_ctx* c, int itime) {
   if (c->slab) {
     const SlabLinks l = slab_links(c, (int)(c->step & 1), (int)((c->step + 1) & 1));
     CK(launch_slab(c->A, c->B, l, c->omega, c->scale, c->p.les_cs, c->st));
+    if (c->g.nz > 2) c->launches++;  // edge planes and interior are two launches
   } else if (c->scheme == BGK_TWO_LATTICE) {
     CK(launch_two_lattice(c->A, c->B, c->omega, c->scale, c->p.les_cs, c->p.kernel, c->st));
   }
@@ -1307,6 +1310,27 @@ int bgk_synchronize(bgk_ctx* c) {
   if (rc) return rc;
   CK(cudaSetDevice(c->p.device));
   return sync_and_check(c);
+}
+
+int bgk_record_event(bgk_ctx* c) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  CK(cudaSetDevice(c->p.device));
+  if (!c->mark) CK(cudaEventCreateWithFlags(&c->mark, cudaEventDisableTiming));
+  CK(cudaEventRecord(c->mark, c->st));
+  return BGK_OK;
+}
+
+int bgk_wait_event(bgk_ctx* c, const bgk_ctx* other) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!other || !other->mark) {
+    set_err("bgk_wait_event: the other context has recorded no event (bgk_record_event)");
+    return BGK_ERR_STATE;
+  }
+  CK(cudaSetDevice(c->p.device));
+  CK(cudaStreamWaitEvent(c->st, other->mark, 0));
+  return BGK_OK;
 }
 
 int bgk_shift3(const void* in1, const void* in2, const void* in3, void* out1, void* out2, void* out3, int nx, int ny,

@@ -290,13 +290,18 @@ __global__ void __launch_bounds__(256) k_aa(Pops<typename F::S> a, Geo g, StepK 
 // stored straight into the neighbour's ghost plane for the next step (a peer
 // store over NVLink when the neighbour is another GPU): the halo exchange of
 // SRC/bcond.comm.step3.F90:77-297 fused into the producing kernel.
-template <class F, bool LES = false>
+// EDGE = false: the interior planes 1..nz-2 (blockIdx.z + 1), whose pulls stay
+// inside the slab (the whole-box kernel's code without the z wrap); EDGE =
+// true: planes 0 and nz-1 (blockIdx.z = 0, 1), which read ghost planes and
+// feed the neighbours. Separate kernels keep the interior one's registers
+// (and so its occupancy) those of the whole-box kernel.
+template <class F, bool LES, bool EDGE>
 __global__ void __launch_bounds__(256) k_slab(Pops<const typename F::S> src, Pops<typename F::S> dst, Geo g,
                                               StepK K, Halo<typename F::S> h) {
   using S = typename F::S;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = blockIdx.z;
+  const int k = EDGE ? (blockIdx.z == 0 ? 0 : g.nz - 1) : (int)blockIdx.z + 1;
   if (i >= g.nx || j >= g.ny) return;
   const int im = i == 0 ? g.nx - 1 : i - 1, ip = i == g.nx - 1 ? 0 : i + 1;
   const int jm = j == 0 ? g.ny - 1 : j - 1, jp = j == g.ny - 1 ? 0 : j + 1;
@@ -306,8 +311,8 @@ __global__ void __launch_bounds__(256) k_slab(Pops<const typename F::S> src, Pop
     const int ii = cxq(q) > 0 ? im : (cxq(q) < 0 ? ip : i);
     const int jj = cyq(q) > 0 ? jm : (cyq(q) < 0 ? jp : j);
     const int po = ii + g.sx * jj;
-    if (czq(q) > 0 && k == 0) v[q] = ldg(h.in_lo[zslot(q)] + po);
-    else if (czq(q) < 0 && k == g.nz - 1) v[q] = ldg(h.in_hi[zslot(q)] + po);
+    if (EDGE && czq(q) > 0 && k == 0) v[q] = ldg(h.in_lo[zslot(q)] + po);
+    else if (EDGE && czq(q) < 0 && k == g.nz - 1) v[q] = ldg(h.in_hi[zslot(q)] + po);
     else {
       const int off = po + g.sx * g.ny * (k - czq(q));
       v[q] = (q == Q - 1) ? src.p[Q - 1][off] : ldg(src.p[q] + off);
@@ -318,18 +323,20 @@ __global__ void __launch_bounds__(256) k_slab(Pops<const typename F::S> src, Pop
   const int o = po + g.sx * g.ny * k;
 #pragma unroll
   for (int q = 0; q < Q; ++q) dst.p[q][o] = v[q];
-  if (k == g.nz - 1) {
+  if (EDGE) {
+    if (k == g.nz - 1) {
 #pragma unroll
-    for (int q = 0; q < Q; ++q)
-      if (czq(q) > 0) h.up[zslot(q)][po] = v[q];
-  }
-  if (k == 0) {
+      for (int q = 0; q < Q; ++q)
+        if (czq(q) > 0) h.up[zslot(q)][po] = v[q];
+    }
+    if (k == 0) {
 #pragma unroll
-    for (int q = 0; q < Q; ++q)
-      if (czq(q) < 0) h.dn[zslot(q)][po] = v[q];
+      for (int q = 0; q < Q; ++q)
+        if (czq(q) < 0) h.dn[zslot(q)][po] = v[q];
+    }
+    // peer stores are made visible system-wide before the thread ends
+    __threadfence_system();
   }
-  // peer stores are made visible system-wide before the thread ends
-  if (k == 0 || k == g.nz - 1) __threadfence_system();
 }
 
 // Fills the neighbours' ghost planes from this slab's current boundary planes
@@ -967,8 +974,16 @@ static cudaError_t slab_impl(const Lattice& s, const Lattice& d, const StepK& K,
   Pops<S> pd = pops_of<S>(d);
   pd.p[Q - 1] = (S*)s.p[Q - 1];  // pop 19 in place (SRC/col_MC.F90:351)
   const Shape sh = cell_shape(s.g);
-  if (K.les) k_slab<F, true><<<sh.grid, sh.block, 0, st>>>(ps, pd, s.g, K, halo_of<S>(&l));
-  else k_slab<F, false><<<sh.grid, sh.block, 0, st>>>(ps, pd, s.g, K, halo_of<S>(&l));
+  const Halo<S> h = halo_of<S>(&l);
+  // planes 0 and nz-1 (one plane when nz = 1), then the interior
+  const dim3 ge(sh.grid.x, sh.grid.y, s.g.nz > 1 ? 2 : 1);
+  if (K.les) k_slab<F, true, true><<<ge, sh.block, 0, st>>>(ps, pd, s.g, K, h);
+  else k_slab<F, false, true><<<ge, sh.block, 0, st>>>(ps, pd, s.g, K, h);
+  if (s.g.nz > 2) {
+    const dim3 gi(sh.grid.x, sh.grid.y, s.g.nz - 2);
+    if (K.les) k_slab<F, true, false><<<gi, sh.block, 0, st>>>(ps, pd, s.g, K, h);
+    else k_slab<F, false, false><<<gi, sh.block, 0, st>>>(ps, pd, s.g, K, h);
+  }
   return cudaGetLastError();
 }
 

@@ -9,7 +9,8 @@ barrier between steps (the library's contract, ``include/bgk3d.h``
 "z-slabs"). Two drivers:
 
 - ``LocalSlabs``: every slab in this process (one or several devices); the
-  barrier synchronises the slabs' streams.
+  barrier is device-side: each slab's stream waits for the events its two
+  neighbours recorded after their step (no host wait).
 - ``DistSlabs``: one slab per process under ``torch.distributed`` (one
   process per GPU). The ghost buffers are shared as CUDA IPC handles
   (``all_gather_object``); the barrier is a one-element all-reduce on the
@@ -116,6 +117,17 @@ class LocalSlabs:
             s.close()
 
     def barrier(self):
+        """Each slab's next work waits, on the device, for its neighbours'
+        queued work (they read and write each other's ghost planes)."""
+        for s in self.slabs:
+            s.record_event()
+        for r, s in enumerate(self.slabs):
+            lo, hi = neighbours(r, self.proc_z)
+            s.wait_event(self.slabs[lo])
+            if hi != lo:
+                s.wait_event(self.slabs[hi])
+
+    def synchronize(self):
         for s in self.slabs:
             s.synchronize()
 

@@ -239,6 +239,14 @@ class BGK3D:
     def synchronize(self):
         check(self._lib.bgk_synchronize(self._h), "bgk_synchronize")
 
+    def record_event(self):
+        """Marks the work queued so far on this context's stream."""
+        check(self._lib.bgk_record_event(self._h), "bgk_record_event")
+
+    def wait_event(self, other: "BGK3D"):
+        """This context's later work waits for `other`'s last marked work."""
+        check(self._lib.bgk_wait_event(self._h, other._h), "bgk_wait_event")
+
     # ---------------------------------------------------------- z-slabs
     # The halo exchange of SRC/bcond.comm.step3.F90 for a box split along z
     # (proc_z > 1); the orchestration across slabs is in slabs.py.

@@ -240,6 +240,12 @@ int bgk_get_launch_count(const bgk_ctx* ctx, long long* count);
 void* bgk_get_stream(const bgk_ctx* ctx);
 /* Waits for all work of the context. */
 int bgk_synchronize(bgk_ctx* ctx);
+/* Device-side ordering between contexts of one process (on one or several
+   devices), without a host wait: bgk_record_event marks the work queued so
+   far on ctx's stream; bgk_wait_event makes ctx's later work wait for the
+   work `other` had queued at its last bgk_record_event. */
+int bgk_record_event(bgk_ctx* ctx);
+int bgk_wait_event(bgk_ctx* ctx, const bgk_ctx* other);
 
 /* z-slabs (proc_z > 1): the halo exchange of bcond_comm_step3
    (SRC/bcond.comm.step3.F90:77-297, five populations per z face) without
@@ -261,7 +267,9 @@ int bgk_synchronize(bgk_ctx* ctx);
         different slabs, every slab's previous call must have completed on the
         device before any slab's next call starts (a barrier: a stream-ordered
         collective such as a one-element NCCL all-reduce on the contexts'
-        streams, or bgk_synchronize on every slab plus a host barrier).
+        streams; in one process, bgk_record_event on every slab and then
+        bgk_wait_event of each slab on its two neighbours; or
+        bgk_synchronize on every slab plus a host barrier).
    bgk_col_mc then advances one slab by one step (bgk_run accepts nsteps <= 1),
    the diagnostics return this slab's contribution to the global means (sums
    divided by the global cell count: the global value is the sum over the

@@ -302,40 +302,47 @@ __global__ void __launch_bounds__(256) k_slab(Pops<const typename F::S> src, Pop
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int k = EDGE ? (blockIdx.z == 0 ? 0 : g.nz - 1) : (int)blockIdx.z + 1;
-  if (i >= g.nx || j >= g.ny) return;
-  const int im = i == 0 ? g.nx - 1 : i - 1, ip = i == g.nx - 1 ? 0 : i + 1;
-  const int jm = j == 0 ? g.ny - 1 : j - 1, jp = j == g.ny - 1 ? 0 : j + 1;
-  S v[Q];
+  const bool active = i < g.nx && j < g.ny;
+  if (!EDGE && !active) return;
+  if (active) {
+    const int im = i == 0 ? g.nx - 1 : i - 1, ip = i == g.nx - 1 ? 0 : i + 1;
+    const int jm = j == 0 ? g.ny - 1 : j - 1, jp = j == g.ny - 1 ? 0 : j + 1;
+    S v[Q];
 #pragma unroll
-  for (int q = 0; q < Q; ++q) {
-    const int ii = cxq(q) > 0 ? im : (cxq(q) < 0 ? ip : i);
-    const int jj = cyq(q) > 0 ? jm : (cyq(q) < 0 ? jp : j);
-    const int po = ii + g.sx * jj;
-    if (EDGE && czq(q) > 0 && k == 0) v[q] = ldg(h.in_lo[zslot(q)] + po);
-    else if (EDGE && czq(q) < 0 && k == g.nz - 1) v[q] = ldg(h.in_hi[zslot(q)] + po);
-    else {
-      const int off = po + g.sx * g.ny * (k - czq(q));
-      v[q] = (q == Q - 1) ? src.p[Q - 1][off] : ldg(src.p[q] + off);
+    for (int q = 0; q < Q; ++q) {
+      const int ii = cxq(q) > 0 ? im : (cxq(q) < 0 ? ip : i);
+      const int jj = cyq(q) > 0 ? jm : (cyq(q) < 0 ? jp : j);
+      const int po = ii + g.sx * jj;
+      if (EDGE && czq(q) > 0 && k == 0) v[q] = ldg(h.in_lo[zslot(q)] + po);
+      else if (EDGE && czq(q) < 0 && k == g.nz - 1) v[q] = ldg(h.in_hi[zslot(q)] + po);
+      else {
+        const int off = po + g.sx * g.ny * (k - czq(q));
+        v[q] = (q == Q - 1) ? src.p[Q - 1][off] : ldg(src.p[q] + off);
+      }
     }
-  }
-  F::template cell<LES>(v, K);
-  const int po = i + g.sx * j;
-  const int o = po + g.sx * g.ny * k;
+    F::template cell<LES>(v, K);
+    const int po = i + g.sx * j;
+    const int o = po + g.sx * g.ny * k;
 #pragma unroll
-  for (int q = 0; q < Q; ++q) dst.p[q][o] = v[q];
-  if (EDGE) {
-    if (k == g.nz - 1) {
+    for (int q = 0; q < Q; ++q) dst.p[q][o] = v[q];
+    if (EDGE && k == g.nz - 1) {
 #pragma unroll
       for (int q = 0; q < Q; ++q)
         if (czq(q) > 0) h.up[zslot(q)][po] = v[q];
     }
-    if (k == 0) {
+    if (EDGE && k == 0) {
 #pragma unroll
       for (int q = 0; q < Q; ++q)
         if (czq(q) < 0) h.dn[zslot(q)][po] = v[q];
     }
-    // peer stores are made visible system-wide before the thread ends
-    __threadfence_system();
+  }
+  if (EDGE) {
+    // the block's stores into the neighbour's planes (peer memory when the
+    // neighbour is another GPU) are made visible system-wide before the
+    // kernel ends: a block barrier, then one system-scope fence (cumulative
+    // over the stores the barrier ordered before it)
+    __syncthreads();
+    if (threadIdx.x == 0 && threadIdx.y == 0) __threadfence_system();
   }
 }
 
@@ -345,15 +352,17 @@ template <class S>
 __global__ void k_halo_prime(Pops<const S> a, Geo g, Halo<S> h) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y;
-  if (i >= g.nx) return;
-  const int po = i + g.sx * j;
-  const long long top = po + (long long)g.sx * g.ny * (g.nz - 1);
+  if (i < g.nx) {
+    const int po = i + g.sx * j;
+    const long long top = po + (long long)g.sx * g.ny * (g.nz - 1);
 #pragma unroll
-  for (int q = 0; q < Q; ++q) {
-    if (czq(q) > 0) h.up[zslot(q)][po] = a.p[q][top];
-    if (czq(q) < 0) h.dn[zslot(q)][po] = a.p[q][po];
+    for (int q = 0; q < Q; ++q) {
+      if (czq(q) > 0) h.up[zslot(q)][po] = a.p[q][top];
+      if (czq(q) < 0) h.dn[zslot(q)][po] = a.p[q][po];
+    }
   }
-  __threadfence_system();
+  __syncthreads();
+  if (threadIdx.x == 0) __threadfence_system();
 }
 
 // ------------------------------------------------------ initial conditions

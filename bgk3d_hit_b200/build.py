@@ -1,4 +1,5 @@
-"""Builds the CUDA library ``libbgk3d.so`` in-tree for sm_100a.
+"""Builds the CUDA library ``libbgk3d.so`` in-tree for sm_100a, and the
+program driver ``bgk3d_hit`` (the reference's main loop over the C-ABI).
 
     python -m bgk3d_hit_b200.build [--force] [--verbose]
 
@@ -41,6 +42,27 @@ def command(out: str = OUT, extra=()) -> list[str]:
     ]
 
 
+DRIVER = os.path.join(HERE, "bgk3d_hit")
+
+
+def driver_command(out: str = DRIVER) -> list[str]:
+    """g++ for the program driver (csrc/driver.cpp) over the C-ABI."""
+    cxx = shutil.which("g++") or "g++"
+    return [cxx, "-O2", "-std=c++17", f"-I{INCLUDE}", os.path.join(CSRC, "driver.cpp"), "-o", out,
+            f"-L{HERE}", "-lbgk3d", "-Wl,-rpath,$ORIGIN"]
+
+
+def build_driver(force: bool = False) -> str:
+    src = os.path.join(CSRC, "driver.cpp")
+    if force or not os.path.exists(DRIVER) or max(os.path.getmtime(src), os.path.getmtime(OUT)) > os.path.getmtime(
+            DRIVER):
+        r = subprocess.run(driver_command(), capture_output=True, text=True)
+        if r.returncode:
+            sys.stderr.write(r.stdout + r.stderr)
+            raise RuntimeError("g++ failed on driver.cpp")
+    return DRIVER
+
+
 def _stale(out: str) -> bool:
     if not os.path.exists(out):
         return True
@@ -69,3 +91,4 @@ if __name__ == "__main__":
     ap.add_argument("--verbose", action="store_true")
     a = ap.parse_args()
     print(build(a.force, a.verbose))
+    print(build_driver(a.force))

@@ -273,6 +273,20 @@ class BGK3D:
         check(self._lib.bgk_halo_prime(self._h), "bgk_halo_prime")
 
 
+def fortran_e(x: float) -> str:
+    """Fortran E14.6 edit descriptor (0.ddddddE+ee, right-justified), the
+    number format of diagno.dat and dissipation.dat."""
+    x = float(x)
+    if not np.isfinite(x):
+        return "%14s" % ("NaN" if np.isnan(x) else ("Infinity" if x > 0 else "-Infinity"))
+    if x == 0.0:
+        return "%14s" % "0.000000E+00"
+    s = "%.5E" % abs(x)
+    e = int(s[8:]) + 1
+    body = "%s0.%s%sE%s%02d" % ("-" if x < 0 else "", s[0], s[2:7], "-" if e < 0 else "+", abs(e))
+    return "%14s" % body
+
+
 def run_loop(box: BGK3D, itfin: int, out_dir: str | None = None, itstart: int = 1, ivtim: int | None = None,
              itsave: int | None = None):
     """Replays the time loop of SRC/bgk3d_HIT.F90:127-146 (boundaries, col_MC,
@@ -308,8 +322,9 @@ def run_loop(box: BGK3D, itfin: int, out_dir: str | None = None, itstart: int = 
                 open(os.path.join(out_dir, "dissipation.dat"), "w") as f71:
             for d in recs:
                 # format 1004: i8, 5(e14.6,1x) -- itime, xtot, ytot, ztot, rtot, stot
-                f70.write("%8d" % d["itime"] + "".join(" %14.6E" % x for x in (
+                # (SRC/diagno.F90:137,152); i8, 4(e14.6,1x) (SRC/dissipation.F90:265-278)
+                f70.write("%8d" % d["itime"] + "".join(fortran_e(x) + " " for x in (
                     d["ux_mean"], d["uy_mean"], d["uz_mean"], d["rho_mean"], d["ke_mean"])) + "\n")
-                f71.write("%8d" % d["itime"] + "".join(" %14.6E" % x for x in (
+                f71.write("%8d" % d["itime"] + "".join(fortran_e(x) + " " for x in (
                     d["t"], d["tke_norm"], d["diss"])) + "\n")
     return recs

@@ -130,3 +130,36 @@ def test_hit_generator_properties():
     e = sum(np.abs(np.fft.fftn(a)) ** 2 for a in (u, v, w))
     shells = np.bincount(np.rint(k).astype(int).ravel(), e.ravel())
     assert abs(int(np.argmax(shells)) - 4) <= 1
+
+
+def test_fortran_e14_6_format():
+    """diagno.dat / dissipation.dat numbers are written as Fortran E14.6."""
+    from bgk3d_hit_b200.solver import fortran_e
+
+    assert fortran_e(0.0123456) == "  0.123456E-01"
+    assert fortran_e(-1.5) == " -0.150000E+01"
+    assert fortran_e(1.0) == "  0.100000E+01"
+    assert fortran_e(0.0) == "  0.000000E+00"
+    assert fortran_e(0.0099999996) == "  0.100000E-01"
+    assert fortran_e(123456789.0) == "  0.123457E+09"
+    assert fortran_e(float("nan")).strip() == "NaN"
+    assert all(len(fortran_e(x)) == 14 for x in (1e-30, -3.3e7, 2.5))
+
+
+def test_driver_builds_and_rejects_bad_input(tmp_path):
+    """The C++ program driver (the reference's main loop over the C-ABI)
+    builds with g++ and reports a missing or inconsistent namelist before it
+    touches a device."""
+    import subprocess
+
+    from bgk3d_hit_b200 import build as B
+
+    exe = B.build_driver()
+    r = subprocess.run([exe, str(tmp_path / "missing.input")], capture_output=True, text=True)
+    assert r.returncode == 2 and "cannot open" in r.stderr
+    nl = tmp_path / "bgk.input"
+    nl.write_text("&parameters\nlx = 16\nproc_z = 2 /\n")
+    r = subprocess.run([exe, str(nl)], capture_output=True, text=True)
+    assert r.returncode == 2 and "one box per process" in r.stderr
+    r = subprocess.run([exe, "--help"], capture_output=True, text=True)
+    assert r.returncode == 0 and "usage" in r.stdout

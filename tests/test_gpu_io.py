@@ -122,3 +122,29 @@ def test_run_loop_writes_slices_and_restarts(bgk, tmp_path):
             assert f"tec_{tag}.00000.{it:08d}.vtk" in names
     assert "restart.00000005.bin" in names and "restart.00000010.bin" in names
     box.close()
+
+
+def test_program_driver_matches_run_loop(bgk, tmp_path):
+    """The C++ driver bgk3d_hit (namelist in, diagno.dat / dissipation.dat /
+    VTK / restarts out) writes the same files as run_loop for the same run."""
+    import subprocess
+
+    from bgk3d_hit_b200 import build as B
+    from bgk3d_hit_b200 import run_loop
+
+    exe = B.build_driver()
+    (tmp_path / "c").mkdir()
+    (tmp_path / "py").mkdir()
+    nl = tmp_path / "bgk.input"
+    nl.write_text("&parameters\nlx = 16\nly = 12\nlz = 10\nu0 = 0.05\nsvisc = 0.01\n"
+                  "itfin = 20\nitsave = 10\nivtim = 10\nicheck = 5 /\n")
+    r = subprocess.run([exe, str(nl), "--out", str(tmp_path / "c")], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    assert "GLUPS" in r.stdout
+    box = bgk.BGK3D.from_input(str(nl), mode="faithful")
+    box.init()
+    run_loop(box, 20, str(tmp_path / "py"), ivtim=10, itsave=10)
+    box.close()
+    for name in ("diagno.dat", "dissipation.dat", "tec_xy.00000.00000010.vtk", "restart.00000020.bin"):
+        assert (tmp_path / "c" / name).read_bytes() == (tmp_path / "py" / name).read_bytes(), name
+    assert (tmp_path / "c" / "bgk.perf").exists()

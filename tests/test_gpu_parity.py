@@ -48,6 +48,28 @@ def test_two_lattice_bitexact_vs_oracle(bgk, oracle_mod, form, shape):
     box.close()
 
 
+@pytest.mark.parametrize("form", ["fp64", "fp32", "fp16"])
+@pytest.mark.parametrize("scheme", ["two_lattice", "aa"])
+def test_hit64_bitexact_vs_oracle(bgk, oracle_mod, form, scheme):
+    """64^3 decaying-HIT initial condition (k0 = 4, u_rms = 0.03), 1 and 10
+    steps, every form and scheme: the oracle's bits."""
+    from bgk3d_hit_b200.hit import hit_velocity
+
+    n = 64
+    u = hit_velocity(n, 4, 0.03, 1234)
+    orc = oracle_mod.OracleLattice(n, n, n, form=FORMS[form], scale=F16_SCALE)
+    orc.init_velocity(*u)
+    box = bgk.BGK3D(n, svisc=0.005 / 3, precision=form, scheme=scheme,
+                    fp16_scale=F16_SCALE if form == "fp16" else 0.0)
+    box.init_velocity(*u)
+    for it in range(1, 11):
+        orc.step(0.005 / 3, periodic=True)
+        box.col_MC(it)
+        if it in (1, 10):
+            assert same_bits(box.populations(), orc.get_pops()), f"after {it} steps"
+    box.close()
+
+
 @pytest.mark.parametrize("kernel", [1, 2, 4])
 @pytest.mark.parametrize("shape", [(64, 64, 64), (32, 16, 8), (8, 8, 8), (256, 4, 4), (128, 6, 5), (24, 8, 6)])
 def test_fp16_kernel_variants_bitexact(bgk, oracle_mod, kernel, shape):

@@ -253,8 +253,8 @@ __global__ void __launch_bounds__(256, 4) k_two_f16v2(Pops<const __half> src, Po
 // Each thread reads exactly the locations it writes, so the update is
 // race-free in place; a location is never read after it has been written,
 // which also makes the read-only load path safe.
-template <class F, bool ODD, bool LES = false>
-__global__ void __launch_bounds__(256) k_aa(Pops<typename F::S> a, Geo g, StepK K) {
+template <class F, bool ODD, bool LES>
+__device__ __forceinline__ void aa_cell(Pops<typename F::S>& a, const Geo& g, const StepK& K) {
   using S = typename F::S;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
@@ -280,6 +280,18 @@ __global__ void __launch_bounds__(256) k_aa(Pops<typename F::S> a, Geo g, StepK 
     if (ODD) a.p[q][back(oppq(q))] = v[q];
     else a.p[oppq(q)][o] = v[q];
   }
+}
+
+template <class F, bool ODD, bool LES = false>
+__global__ void __launch_bounds__(256) k_aa(Pops<typename F::S> a, Geo g, StepK K) {
+  aa_cell<F, ODD, LES>(a, g, K);
+}
+
+// The FP16 odd step (BGK) is latency-bound on registers: capped at 48 (5
+// blocks per SM) it measured 53.7 against 50.4 GLUPS uncapped for that step at
+// 256^3 on B200, a few spilled bytes included.
+__global__ void __launch_bounds__(256, 5) k_aa_f16_odd(Pops<__half> a, Geo g, StepK K) {
+  aa_cell<F16, true, false>(a, g, K);
 }
 
 // ----------------------------------------------------------------- z-slabs
@@ -838,7 +850,9 @@ static cudaError_t aa_impl(const Lattice& a, int odd, const StepK& K, int varian
     cudaError_t e = launch_rows(a, a, odd ? ROW_AA_ODD : ROW_AA_EVEN, K, st, &launched);
     if (e != cudaSuccess || launched) return e;
   }
-  if (odd) k_aa<F, true><<<sh.grid, sh.block, 0, st>>>(pops_of<S>(a), a.g, K);
+  if (odd && F::id == FORM_F16)
+    k_aa_f16_odd<<<sh.grid, sh.block, 0, st>>>(pops_of<__half>(a), a.g, K);
+  else if (odd) k_aa<F, true><<<sh.grid, sh.block, 0, st>>>(pops_of<S>(a), a.g, K);
   else k_aa<F, false><<<sh.grid, sh.block, 0, st>>>(pops_of<S>(a), a.g, K);
   return cudaGetLastError();
 }

@@ -147,11 +147,14 @@ struct F32 {
 // directly, keeps the density deviation dr = sum(f - w) apart from 1, treats
 // each pair of opposite directions together and uses fused multiply-adds:
 //   dr = sum(y)/scale, u = j(y)/(scale*(1 + dr)), a = -1.5|u|^2,
-//   for the pair (q, opp q) with cu = c_q.u:
-//     Q2 = (4.5 cu) cu + a,  P(+-) = +-3 cu + Q2   (f_eq/w - 1 = dr + (1+dr) P)
-//   y' = (1 - omega) y + kd + kr P, kd = K dr, kr = K + kd, K = omega*scale*w.
-// Sums and roundings are fixed (moments16, pair16) and restated by the oracle.
-struct Mom16 { float dr, ux, uy, uz, a, kd[3], kr[3]; };
+//   P(+-) = +-3 cu + 4.5 cu^2 + a for the pair (q, opp q), cu = c_q.u
+//   (f_eq/w - 1 = dr + (1+dr) P), and
+//   y' = (1 - omega) y + K dr + K (1 + dr) P, K = omega*scale*w,
+// regrouped per weight class with kr = K + K dr:
+//   t = (4.5 kr cu) cu + (kr a + K dr),  y'(+-) = (1 - omega) y + t +- 3 kr cu
+// (six fused operations per pair). Sums and roundings are fixed (moments16,
+// pair16) and restated by the oracle.
+struct Mom16 { float dr, ux, uy, uz, a, kr3[3], kr45[3], kra[3]; };
 
 __device__ __forceinline__ Mom16 moments16(const float (&y)[Q], const StepK& k) {
   const float sp = __fadd_rn(__fadd_rn(__fadd_rn(y[0], y[1]), __fadd_rn(y[2], y[3])), y[4]);
@@ -168,7 +171,9 @@ __device__ __forceinline__ Mom16 moments16(const float (&y)[Q], const StepK& k) 
   Mom16 m;
   const float dr = __fmul_rn(sum, k.inv);
   m.dr = dr;
-  const float r = __fdiv_rn(k.inv, __fadd_rn(1.0f, dr));
+  // inv/(1 + dr) as inv * rcp(1 + dr): inv is a power of two, so scaling the
+  // correctly rounded reciprocal is exact and the result equals the division
+  const float r = __fmul_rn(k.inv, __frcp_rn(__fadd_rn(1.0f, dr)));
   m.ux = __fmul_rn(jx, r);
   m.uy = __fmul_rn(__fsub_rn(jyp, jym), r);
   m.uz = __fmul_rn(__fsub_rn(jzp, jzm), r);
@@ -176,8 +181,11 @@ __device__ __forceinline__ Mom16 moments16(const float (&y)[Q], const StepK& k) 
   m.a = __fmul_rn(-1.5f, usq);
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
-    m.kd[c] = __fmul_rn(k.kw[c], dr);
-    m.kr[c] = __fadd_rn(k.kw[c], m.kd[c]);
+    const float kd = __fmul_rn(k.kw[c], dr);
+    const float kr = __fadd_rn(k.kw[c], kd);
+    m.kr3[c] = __fmul_rn(3.0f, kr);
+    m.kr45[c] = __fmul_rn(4.5f, kr);
+    m.kra[c] = __fmaf_rn(kr, m.a, kd);
   }
   return m;
 }
@@ -197,16 +205,14 @@ __device__ __forceinline__ float cdotu(int q, const Mom16& m) {
 __device__ __forceinline__ void pair16(int q, float yq, float yo, const Mom16& m, float om1, float& oq, float& oo) {
   const int c = wclass(q);
   const float cu = cdotu(q, m);
-  const float q2 = __fmaf_rn(__fmul_rn(4.5f, cu), cu, m.a);
-  const float pp = __fmaf_rn(3.0f, cu, q2);
-  const float pm = __fmaf_rn(-3.0f, cu, q2);
-  oq = __fmaf_rn(m.kr[c], pp, __fmaf_rn(om1, yq, m.kd[c]));
-  oo = __fmaf_rn(m.kr[c], pm, __fmaf_rn(om1, yo, m.kd[c]));
+  const float t = __fmaf_rn(__fmul_rn(m.kr45[c], cu), cu, m.kra[c]);
+  oq = __fmaf_rn(m.kr3[c], cu, __fmaf_rn(om1, yq, t));
+  oo = __fmaf_rn(-m.kr3[c], cu, __fmaf_rn(om1, yo, t));
 }
 
 // Rest population (cu = 0, P = a).
 __device__ __forceinline__ float rest16(float y, const Mom16& m, float om1) {
-  return __fmaf_rn(m.kr[0], m.a, __fmaf_rn(om1, y, m.kd[0]));
+  return __fmaf_rn(om1, y, m.kra[0]);
 }
 
 // FP16 form with the Smagorinsky closure: per cell, Pi_neq from the

@@ -305,8 +305,13 @@ double FN(orc_omega)(double svisc) {
    multiply-adds (C fmaf, correctly rounded):
      dr = sum(y)*inv, u = j(y)*(inv/(1 + dr)), a = -1.5|u|^2,
      kd = K*dr, kr = K + kd with K = omega*scale*w (per weight class),
-     Q2 = fmaf(4.5*cu, cu, a), P(+-) = fmaf(+-3, cu, Q2),
-     y' = fmaf(kr, P, fmaf(1 - omega, y, kd)).
+     kr3 = 3*kr, kr45 = 4.5*kr, kra = fmaf(kr, a, kd),
+     t = fmaf(kr45*cu, cu, kra),
+     y'(q) = fmaf(kr3, cu, fmaf(1 - omega, y, t)),
+     y'(opp q) = fmaf(-kr3, cu, fmaf(1 - omega, y, t)),
+     y'(rest) = fmaf(1 - omega, y, kra)
+   (the BGK update y' = (1 - omega) y + K dr + K(1 + dr)(+-3cu + 4.5cu^2 + a)
+   regrouped).
    The sums are grouped as written; this is the definition the CUDA kernels
    follow operation for operation. */
 static inline float FN(cdotu16)(int q, float ux, float uy, float uz) {
@@ -336,17 +341,21 @@ static void FN(fast16_cell)(const float *y, float *out, float inv, float om1, co
     const float ux = jx * r, uy = (jyp - jym) * r, uz = (jzp - jzm) * r;
     const float usq = fmaf(uz, uz, fmaf(uy, uy, ux * ux));
     const float a = -1.5f * usq;
-    float kd[3], kr[3];
-    for (int c = 0; c < 3; ++c) { kd[c] = kw[c] * dr; kr[c] = kw[c] + kd[c]; }
+    float kr3[3], kr45[3], kra[3];
+    for (int c = 0; c < 3; ++c) {
+        const float kd = kw[c] * dr, kr = kw[c] + kd;
+        kr3[c] = 3.0f * kr;
+        kr45[c] = 4.5f * kr;
+        kra[c] = fmaf(kr, a, kd);
+    }
     for (int q = 0; q < 9; ++q) {
         const int c = wcls[q], o = opp[q];
         const float cu = FN(cdotu16)(q, ux, uy, uz);
-        const float q2 = fmaf(4.5f * cu, cu, a);
-        const float pp = fmaf(3.0f, cu, q2), pm = fmaf(-3.0f, cu, q2);
-        out[q] = fmaf(kr[c], pp, fmaf(om1, y[q], kd[c]));
-        out[o] = fmaf(kr[c], pm, fmaf(om1, y[o], kd[c]));
+        const float t = fmaf(kr45[c] * cu, cu, kra[c]);
+        out[q] = fmaf(kr3[c], cu, fmaf(om1, y[q], t));
+        out[o] = fmaf(-kr3[c], cu, fmaf(om1, y[o], t));
     }
-    out[18] = fmaf(kr[0], a, fmaf(om1, y[18], kd[0]));
+    out[18] = fmaf(om1, y[18], kra[0]);
 }
 
 /* The FP16 form with the Smagorinsky closure (the reference's LES block,

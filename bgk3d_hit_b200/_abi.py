@@ -77,6 +77,7 @@ PROTOTYPES = [
     ("bgk_load", _i, [_vp, C.c_char_p]),
     ("bgk_vtk", _i, [_vp, _i, _i, _i, C.c_char_p]),
     ("bgk_adjoint", _i, [_vp, _dp, _dp, _dp, _dp, _dp, _dp, _i, _i, _dp, _dp, _dp]),
+    ("bgk_adjoint_cache", _i, [_vp, C.c_size_t]),
     ("bgk_tangent", _i, [_vp, _dp, _dp, _dp, _dp, _dp, _dp, _d, _dp, _dp, _dp, _i, _dp, _dp]),
     ("bgk_get_scale", _i, [_vp, _dp]),
     ("bgk_get_omega", _i, [_vp, _dp]),

@@ -1,7 +1,7 @@
 """Checks and costs of the discrete adjoint on decaying HIT.
 
     python -m bgk3d_hit_b200.adjoint_study [--size 128] [--steps 1000] [--ckpt 32]
-        [--tau 0.51] [--k0 4] [--dirs 64] [--h 1e-6] [--precision fp64]
+        [--tau 0.51] [--k0 4] [--dirs 64] [--h 1e-6] [--precision fp64] [--cache-gb 0]
 
 Initial velocity: seeded HIT field (seed 1234, E(k) ~ k^4 exp(-2 (k/k0)^2),
 u_rms = 0.03); target u_tgt: the same generator with a second seed (4321).
@@ -12,7 +12,10 @@ Loss = 0.5 mean |u(T) - u_tgt|^2. Reports, as one JSON object:
 - tangent: the relative difference between <grad, d> + grad_tau dtau and the
   tangent-linear derivative along (d, dtau) for a few directions;
 - cost: wall time of the adjoint call (forward with checkpoints, recomputation,
-  backward) over the wall time of a forward-only call of the same length;
+  backward) over the wall time of a forward-only call of the same length
+  (medians of 5 calls each);
+  with --cache-gb G, bgk_adjoint keeps up to G GB of forward states between
+  checkpoints instead of recomputing them (bgk_adjoint_cache);
 - vs_fp64 (FP32 storage only): the relative L2 difference between the FP32
   gradient and the FP64 adjoint gradient of the same problem (central
   differences of an FP32 loss over 1000 steps are dominated by its rounding,
@@ -48,21 +51,31 @@ def _adj(box, u0, ut, T, K, grads):
     return loss.value, g, gt.value
 
 
-def run(size=128, steps=1000, ckpt=32, tau=0.51, k0=4.0, u_rms=0.03, dirs=64, h=1e-6, precision="fp64", ntan=4):
+def run(size=128, steps=1000, ckpt=32, tau=0.51, k0=4.0, u_rms=0.03, dirs=64, h=1e-6, precision="fp64", ntan=4,
+        cache_gb=0.0, reps=5):
     svisc = (tau - 0.5) / 3.0
     u0 = [np.ascontiguousarray(a) for a in hit_velocity(size, k0, u_rms, 1234)]
     ut = [np.ascontiguousarray(a) for a in hit_velocity(size, k0, u_rms, 4321)]
     box = BGK3D(size, svisc=svisc, u0=u_rms, precision=precision)
+    if cache_gb > 0:
+        box._lib.bgk_adjoint_cache(box._h, int(cache_gb * 1e9))
     tau_used = 1.0 / box.omega
-    # cost: forward-only and full adjoint, each timed after one warm-up call
+    # cost: forward-only and full adjoint, each the median of `reps` calls
+    # after one warm-up call
     _adj(box, u0, ut, steps, ckpt, False)
-    t0 = time.perf_counter()
-    loss, _, _ = _adj(box, u0, ut, steps, ckpt, False)
-    t_fwd = time.perf_counter() - t0
+    tf = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        loss, _, _ = _adj(box, u0, ut, steps, ckpt, False)
+        tf.append(time.perf_counter() - t0)
+    t_fwd = float(np.median(tf))
     _adj(box, u0, ut, steps, ckpt, True)
-    t0 = time.perf_counter()
-    loss2, g, gtau = _adj(box, u0, ut, steps, ckpt, True)
-    t_adj = time.perf_counter() - t0
+    ta = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        loss2, g, gtau = _adj(box, u0, ut, steps, ckpt, True)
+        ta.append(time.perf_counter() - t0)
+    t_adj = float(np.median(ta))
     rng = np.random.default_rng(2024)
     errs = []
     for _ in range(dirs):
@@ -103,7 +116,7 @@ def run(size=128, steps=1000, ckpt=32, tau=0.51, k0=4.0, u_rms=0.03, dirs=64, h=
                 "grad_tau_rel": abs(gtau - gt64) / abs(gt64)}
     return {
         "config": {"size": size, "steps": steps, "ckpt_every": ckpt, "tau": tau_used, "k0": k0, "u_rms": u_rms,
-                   "precision": precision, "h": h, "directions": dirs},
+                   "precision": precision, "h": h, "directions": dirs, "cache_gb": cache_gb},
         "loss": loss, "loss_in_adjoint_call": loss2, "grad_tau": gtau, "fd_grad_tau": fd_tau,
         "fd": {"max_rel_err": float(np.max(errs)), "median_rel_err": float(np.median(errs)),
                "p90_rel_err": float(np.percentile(errs, 90)),
@@ -124,8 +137,10 @@ def main():
     ap.add_argument("--dirs", type=int, default=64)
     ap.add_argument("--h", type=float, default=1e-6)
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
+    ap.add_argument("--cache-gb", type=float, default=0.0)
     a = ap.parse_args()
-    print(json.dumps(run(a.size, a.steps, a.ckpt, a.tau, a.k0, dirs=a.dirs, h=a.h, precision=a.precision)))
+    print(json.dumps(run(a.size, a.steps, a.ckpt, a.tau, a.k0, dirs=a.dirs, h=a.h, precision=a.precision,
+                         cache_gb=a.cache_gb)))
 
 
 if __name__ == "__main__":

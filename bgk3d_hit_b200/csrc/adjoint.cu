@@ -80,16 +80,22 @@ __global__ void __launch_bounds__(DIAG_THREADS) k_adj_terminal(Pops<const typena
   acc_block(loss, sh, acc);
 }
 
-// One cell per thread on the forward kernels' launch shape. The adjoint
-// arithmetic runs in the form's arithmetic type R (fused multiply-adds
-// allowed; e_p = w_p (rho (1 + P_p) - 1) from the P_p terms the adjoint needs
-// anyway), the dL/domega terms lam_p (e_p - g_p) are summed in double. lam is
-// read twice (the second time from cache) so that few values stay live. Each
-// block adds its dL/domega contribution (warp shuffles, then the eight warp
-// sums in order) into its own compensated pair acc[2*block].
+// One cell per thread on the forward kernels' launch shape, in one pass over
+// the populations: with wl_p = w_p lam_p, the sums A, B and the dL/domega term
+// need only the moments L0 = sum wl, M1 = sum wl c, M2 = sum wl c c^T and
+// S1 = sum lam g of the cell, because P_p depends on c_p only through c_p.u:
+//   A = L0 (1 + a) + 3 u.M1 + 4.5 u.M2.u,    a = -1.5 |u|^2,
+//   B = 3 (M1 + 3 M2 u - u L0),
+//   sum lam.(e - g) = rho A - L0 - S1.
+// So no population array stays live across the cell. lam is read again from
+// cache for the output. rho and u are formed in the form's arithmetic R, the
+// moment sums and A, B, G in double. Each block adds its dL/domega
+// contribution (warp shuffles, then the eight warp sums in order) into its
+// own compensated pair acc[2*block].
 template <class F>
-__global__ void __launch_bounds__(256, sizeof(typename F::S) == 4 ? 4 : 2) k_adj_step(Pops<const typename F::S> ft, Pops<const typename F::S> lin,
-                                                  Pops<typename F::S> lout, Geo g, typename F::R omega, double* acc) {
+__global__ void __launch_bounds__(256, 2) k_adj_step(Pops<const typename F::S> ft, Pops<const typename F::S> lin,
+                                                     Pops<typename F::S> lout, Geo g, typename F::R omega,
+                                                     double* acc) {
   using S = typename F::S; using R = typename F::R;
   __shared__ double wsum[8];
   double dw = 0.0;
@@ -107,43 +113,48 @@ __global__ void __launch_bounds__(256, sizeof(typename F::S) == 4 ? 4 : 2) k_adj
       const int kk = czq(q) > 0 ? km : (czq(q) < 0 ? kp : k);
       return ii + g.sx * (jj + g.ny * kk);
     };
-    R x[Q];
-#pragma unroll
-    for (int q = 0; q < Q; ++q) x[q] = (R)__ldg(ft.p[q] + offq(q));
     R rho = (R)1, jx = 0, jy = 0, jz = 0;
+    double L0 = 0, m1x = 0, m1y = 0, m1z = 0, mxx = 0, myy = 0, mzz = 0, mxy = 0, mxz = 0, myz = 0, S1 = 0;
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
-      rho += x[q];
-      jx += (R)cxq(q) * x[q];
-      jy += (R)cyq(q) * x[q];
-      jz += (R)czq(q) * x[q];
-    }
-    const R ri = (R)1 / rho, ux = jx * ri, uy = jy * ri, uz = jz * ri;
-    const R a15 = (R)-1.5 * (ux * ux + uy * uy + uz * uz);
-    R A = 0, L0 = 0, Lx = 0, Ly = 0, Lz = 0;
-#pragma unroll
-    for (int q = 0; q < Q; ++q) {
-      const R lam = (R)__ldg(lin.p[q] + o);
-      const R cu = cdot<R>(q, ux, uy, uz);
-      const R P = cu * ((R)3 + (R)4.5 * cu) + a15;
-      const R w = wq<R>(q);
-      const R wl = w * lam;
-      A += wl * ((R)1 + P);
+      const R x = (R)__ldg(ft.p[q] + offq(q));
+      const double lam = (double)__ldg(lin.p[q] + o);
+      rho += x;
+      jx += (R)cxq(q) * x;
+      jy += (R)cyq(q) * x;
+      jz += (R)czq(q) * x;
+      S1 += lam * (double)x;
+      const double wl = wq<double>(q) * lam;
       L0 += wl;
-      const R t = wl * ((R)1 + (R)3 * cu);
-      Lx += t * (R)cxq(q);
-      Ly += t * (R)cyq(q);
-      Lz += t * (R)czq(q);
-      const R e = w * (rho * ((R)1 + P) - (R)1);
-      dw += (double)lam * ((double)e - (double)x[q]);
+      m1x += cxq(q) * wl;
+      m1y += cyq(q) * wl;
+      m1z += czq(q) * wl;
+      mxx += (cxq(q) * cxq(q)) * wl;
+      myy += (cyq(q) * cyq(q)) * wl;
+      mzz += (czq(q) * czq(q)) * wl;
+      mxy += (cxq(q) * cyq(q)) * wl;
+      mxz += (cxq(q) * czq(q)) * wl;
+      myz += (cyq(q) * czq(q)) * wl;
     }
-    const R Bx = (R)3 * (Lx - ux * L0), By = (R)3 * (Ly - uy * L0), Bz = (R)3 * (Lz - uz * L0);
-    const R G = A - (Bx * ux + By * uy + Bz * uz);
+    const R ri = (R)1 / rho;
+    const double ux = (double)(jx * ri), uy = (double)(jy * ri), uz = (double)(jz * ri);
+    const double a = -1.5 * (ux * ux + uy * uy + uz * uz);
+    const double nx = mxx * ux + mxy * uy + mxz * uz;  // M2 u
+    const double ny = mxy * ux + myy * uy + myz * uz;
+    const double nz = mxz * ux + myz * uy + mzz * uz;
+    const double A = L0 * (1.0 + a) + 3.0 * (ux * m1x + uy * m1y + uz * m1z) + 4.5 * (ux * nx + uy * ny + uz * nz);
+    const double Bx = 3.0 * (m1x + 3.0 * nx - ux * L0);
+    const double By = 3.0 * (m1y + 3.0 * ny - uy * L0);
+    const double Bz = 3.0 * (m1z + 3.0 * nz - uz * L0);
+    const double G = A - (Bx * ux + By * uy + Bz * uz);
+    dw = (double)rho * A - L0 - S1;
     const R om1 = (R)1 - omega;
+    const R om = omega;
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
       const R lam = (R)__ldg(lin.p[q] + o);
-      const R mu = om1 * lam + omega * (G + cdot<R>(q, Bx, By, Bz));
+      const R gq = (R)(G + cdot<double>(q, Bx, By, Bz));
+      const R mu = om1 * lam + om * gq;
       lout.p[q][offq(q)] = (S)mu;  // reverse streaming: lam_t,q(x - c_q) = mu_q(x)
     }
   }

@@ -84,6 +84,7 @@ struct bgk_ctx {
   double* adj_acc = nullptr;
   long long adj_acc_n = 0;
   double* adj_tot = nullptr;
+  size_t adj_cache_bytes = 0;  // bgk_adjoint_cache budget
   // z-slab (proc_z > 1): ghost buffer [parity 2][face 2][NZF][plane_elems],
   // the neighbours' buffers, and whether the neighbours' planes were filled
   // from the current state
@@ -1166,6 +1167,16 @@ int bgk_adjoint(bgk_ctx* c, const double* u0, const double* v0, const double* w0
   if ((rc = upload3(c, 1, ut, vt, wt, &dut, "target velocity"))) return rc;
   const long long nacc = adj_step_blocks(c->g) > DIAG_BLOCKS ? adj_step_blocks(c->g) : DIAG_BLOCKS;
   if ((rc = B.sums(nacc, &acc, &tot))) return rc;
+  // segments kept whole in the cache budget (the last ones of the horizon):
+  // segment s holds the states t0+1 .. t1-1 between its checkpoint and the next
+  const size_t state_bytes = (size_t)Q * c->g.qs * c->es;
+  int ncache = 0;
+  if (want_grad && K > 1) {
+    const size_t per_seg = (size_t)(K - 1) * state_bytes;
+    ncache = (int)(c->adj_cache_bytes / per_seg);
+    if (ncache > nck) ncache = nck;
+  }
+  const int s_cache = nck - ncache;  // first cached segment
   std::vector<Lattice> ck(want_grad ? nck : 1), work(want_grad ? nwork : 2), lam(want_grad ? 2 : 1);
   for (auto& L : ck)
     if ((rc = B.lattice(&L, "checkpoint"))) return rc;
@@ -1173,14 +1184,24 @@ int bgk_adjoint(bgk_ctx* c, const double* u0, const double* v0, const double* w0
     if ((rc = B.lattice(&L, "recomputed state"))) return rc;
   for (auto& L : lam)
     if ((rc = B.lattice(&L, "adjoint state"))) return rc;
-  // forward: f^0 = equilibrium of u0 at rho = 1, checkpoints every K steps
+  std::vector<std::vector<Lattice>> cache(nck);
+  for (int s = s_cache; s < nck; ++s) {
+    const int t0 = s * K, t1 = t0 + K < T ? t0 + K : T;
+    cache[s].resize(t1 - t0 - 1);
+    for (auto& L : cache[s])
+      if ((rc = B.lattice(&L, "cached forward state"))) return rc;
+  }
+  // forward: f^0 = equilibrium of u0 at rho = 1, checkpoints every K steps,
+  // the states of cached segments into their slots
   const size_t n = (size_t)ncell(c);
   CK(launch_init_velocity(ck[0], LAY_TWO, du0, du0 + n, du0 + 2 * n, 1.0, 0, c->g.nz, 1.0, nullptr, c->st));
   const Lattice* cur = &ck[0];
   int wi = 0;
   for (int t = 0; t < T; ++t) {
     const Lattice* next;
+    const int s = t / K, m = t + 1 - s * K;  // f^{t+1} is state m of segment s
     if (want_grad && t + 1 < T && (t + 1) % K == 0) next = &ck[(t + 1) / K];
+    else if (want_grad && s >= s_cache && t + 1 < T) next = &cache[s][m - 1];
     else {
       if (cur == &work[wi]) wi ^= 1;
       next = &work[wi];
@@ -1201,14 +1222,19 @@ int bgk_adjoint(bgk_ctx* c, const double* u0, const double* v0, const double* w0
       std::vector<const Lattice*> st(t1 - t0);
       st[0] = &ck[s];
       for (int m = 1; m < t1 - t0; ++m) {
-        CK(launch_step_out_of_place(*st[m - 1], work[m - 1], c->omega, c->st));
-        st[m] = &work[m - 1];
+        if (s >= s_cache) {
+          st[m] = &cache[s][m - 1];  // kept by the forward pass
+        } else {
+          CK(launch_step_out_of_place(*st[m - 1], work[m - 1], c->omega, c->st));
+          st[m] = &work[m - 1];
+          c->launches++;
+        }
       }
       for (int t = t1 - 1; t >= t0; --t) {
         CK(launch_adj_step(*st[t - t0], lam[li], lam[li ^ 1], c->omega, acc, c->st));
         li ^= 1;
       }
-      c->launches += 2 * (t1 - t0) - 1;
+      c->launches += t1 - t0;
     }
     CK(launch_acc_total_n(acc, adj_step_blocks(c->g), tot + 1, c->st));
     if (grad_u0) {
@@ -1224,6 +1250,22 @@ int bgk_adjoint(bgk_ctx* c, const double* u0, const double* v0, const double* w0
   CK(cudaStreamSynchronize(c->st));
   *loss = h[0] / (double)n;
   if (grad_tau) *grad_tau = -c->omega * c->omega * h[1];  // tau = 1/omega
+  return BGK_OK;
+}
+
+int bgk_adjoint_cache(bgk_ctx* c, size_t bytes) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (bytes < c->adj_cache_bytes) {
+    // release the pooled lattices; the next call allocates what it needs
+    CK(cudaSetDevice(c->p.device));
+    CK(cudaStreamSynchronize(c->st));
+    const size_t lb = (size_t)Q * c->g.qs * c->es;
+    for (void* m : c->lat_pool) cudaFree(m);
+    c->dev_bytes -= (long long)(lb * c->lat_pool.size());
+    c->lat_pool.clear();
+  }
+  c->adj_cache_bytes = bytes;
   return BGK_OK;
 }
 

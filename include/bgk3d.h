@@ -218,6 +218,15 @@ int bgk_adjoint(bgk_ctx* ctx, const double* u0, const double* v0, const double* 
                 const double* v_tgt, const double* w_tgt, int nsteps, int ckpt_every, double* loss,
                 double* grad_u0, double* grad_tau);
 
+/* Device memory (bytes, default 0) that bgk_adjoint may spend on keeping the
+   forward states between checkpoints, so that the backward pass need not
+   recompute them: whole segments of ckpt_every - 1 states are kept, the last
+   segments of the horizon first, as many as fit. With the whole horizon kept
+   (ckpt_every - 1 states per segment) the recomputation disappears; results
+   are identical either way. The states stay allocated in the context like the
+   other adjoint buffers; a smaller budget frees them. */
+int bgk_adjoint_cache(bgk_ctx* ctx, size_t bytes);
+
 /* Tangent-linear run (forward-mode derivative) of the same loss: dloss is the
    derivative of loss along the perturbation (du0, dv0, dw0) of the initial
    velocity and dtau of tau. Used to check bgk_adjoint:

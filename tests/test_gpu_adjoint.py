@@ -162,3 +162,28 @@ def test_adjoint_rejects_fp16_and_bad_arguments(bgk):
                               C.byref(loss), None, None)
     assert rc == bgk._abi.BGK_ERR_INVALID
     box.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_adjoint_state_cache_gives_identical_results(bgk, precision):
+    """Keeping forward states (bgk_adjoint_cache) instead of recomputing them
+    changes nothing in the loss or the gradients, whether some or all
+    segments are kept; a budget of 0 frees the kept states."""
+    n, T, K = 12, 17, 4
+    u0, ut = fields(n, 4), fields(n, 5)
+    box = bgk.BGK3D(n, svisc=0.02, precision=precision)
+    ref = adjoint(box, u0, ut, T, K)
+    es = 8 if precision == "fp64" else 4
+    state = 19 * 32 * n * n * es  # rows padded to 32 cells
+    lib = box._lib
+    for budget in (state * (K - 1), 2 * state * (K - 1), 1 << 40):
+        assert lib.bgk_adjoint_cache(box._h, budget) == 0
+        got = adjoint(box, u0, ut, T, K)
+        assert got[0] == ref[0] and got[2] == ref[2]
+        assert np.array_equal(got[1], ref[1])
+    before = box.device_bytes
+    assert lib.bgk_adjoint_cache(box._h, 0) == 0
+    assert box.device_bytes < before
+    got = adjoint(box, u0, ut, T, K)
+    assert np.array_equal(got[1], ref[1])
+    box.close()

@@ -791,11 +791,12 @@ static cudaError_t two_impl(const Lattice& s, const Lattice& d, const StepK& K, 
     cudaError_t e = launch_rows(s, d, ROW_TWO, K, st, &launched);
     if (e != cudaSuccess || launched) return e;
   }
-  // automatic choice (variant 0): one cell per thread, the fastest measured
-  // on B200 for every form at 256^3 (FP16: 62.0 GLUPS vs 61.2 / 62.3 for two /
-  // four cells per thread and 44.6 for the row pipeline)
-  if (F::id == FORM_F16 && (variant == 2 || variant == 4)) {
-    const int V = variant;
+  // automatic choice (variant 0): one cell per thread for FP64 and FP32, four
+  // cells per thread for FP16 where the box fits it - the fastest measured on
+  // B200 at 256^3 (FP16: 64.5 GLUPS with four cells per thread against 64.0
+  // with one, 62.7 with two and 44.6 for the row pipeline)
+  if (F::id == FORM_F16 && (variant == 2 || variant == 4 || variant == 0)) {
+    const int V = variant == 0 ? 4 : variant;
     const int lt = f16v_log_tpr(s.g, V);
     if (lt >= 0) {
       const long long threads = (long long)s.g.ny << lt;

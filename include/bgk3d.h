@@ -82,7 +82,8 @@ typedef struct {
   int use_omega;       /* 1: use `omega` below instead of the svisc formula */
   double omega;        /* collision frequency override (e.g. 0 = pure streaming) */
   int extras;          /* 1: bgk_diagnostic also computes enstrophy */
-  int kernel;          /* stream-collide kernel: 0 automatic, 1 one cell per thread,
+  int kernel;          /* stream-collide kernel: 0 automatic (FP16 two-lattice: 4 where
+                          the box fits, else 1), 1 one cell per thread,
                           2 / 4 two / four cells per thread (FP16 two-lattice), 8 row
                           pipeline with TMA bulk copies into shared memory (rows up to
                           about 5 KB); boxes a kernel does not fit use 1. All give

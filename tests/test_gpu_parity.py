@@ -84,6 +84,23 @@ def test_fp16_kernel_variants_bitexact(bgk, oracle_mod, kernel, shape):
     box.close()
 
 
+@pytest.mark.parametrize("kernel", [0, 1, 4])
+@pytest.mark.parametrize("shape", [(64, 64, 64), (32, 16, 8), (8, 8, 8), (256, 4, 4), (128, 6, 5), (24, 8, 6),
+                                   (512, 2, 3)])
+def test_fp16_aa_kernel_variants_bitexact(bgk, oracle_mod, kernel, shape):
+    """The four-cells-per-thread FP16 AA kernels (x-crossing values moved
+    between lanes on loads and stores; rows inside a warp, one warp and
+    several warps per row; fallback where a box does not fit) give the
+    oracle's bits over steps of both parities."""
+    orc, box = make_pair(bgk, oracle_mod, shape, "fp16", scheme="aa", kernel=kernel)
+    for it in range(1, 6):
+        orc.step(0.01, periodic=True)
+        box.col_MC(it)
+        if it in (1, 2, 5):
+            assert same_bits(box.populations(), orc.get_pops()), f"after {it} steps"
+    box.close()
+
+
 @pytest.mark.parametrize("form", ["fp64", "fp32", "fp16"])
 @pytest.mark.parametrize("scheme", ["two_lattice", "aa"])
 @pytest.mark.parametrize("shape", [(5, 7, 9), (64, 16, 8), (33, 20, 7), (256, 3, 2)])

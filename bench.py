@@ -276,11 +276,11 @@ def run_ours(a):
     achieved = bpc * float(L) ** 3 / per_launch_s / 1e9
     peak, peak_kind = measured_hbm()
     kern = f"{'k_two' if a.scheme == 'two_lattice' else 'k_aa'}_{a.precision}" + ("_les" if a.les_cs > 0 else "")
-    if a.precision == "fp16" and a.scheme == "two_lattice" and a.les_cs == 0 and a.kernel in (0, 2, 4):
+    if a.precision == "fp16" and a.les_cs == 0 and a.kernel in ((0, 2, 4) if a.scheme == "two_lattice" else (0, 4)):
         v = 2 if a.kernel == 2 else 4
         tpr = L // v
-        if L % v == 0 and tpr & (tpr - 1) == 0 and (L * tpr) % 32 == 0:
-            kern = "k_two_f16v2" if a.kernel == 2 else "k_two_f16v"  # cells per thread: 2 or 4
+        if L % v == 0 and tpr & (tpr - 1) == 0 and (L * tpr) % 32 == 0:  # cells per thread: 2 or 4
+            kern = ("k_two_f16v2" if a.kernel == 2 else "k_two_f16v") if a.scheme == "two_lattice" else "k_aa_f16v"
     tr = ncu_traffic(kern)
     traffic = tr * float(L) ** 3 if tr else None
 

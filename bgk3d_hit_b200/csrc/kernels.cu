@@ -929,7 +929,7 @@ static cudaError_t two_impl(const Lattice& s, const Lattice& d, const StepK& K, 
   }
   // automatic choice (variant 0): one cell per thread for FP64 and FP32, four
   // cells per thread for FP16 where the box fits it - the fastest measured on
-  // B200 at 256^3 (FP16: 64.5 GLUPS with four cells per thread against 64.0
+  // B200 at 256^3 (FP16: 76.6 GLUPS with four cells per thread against 64.0
   // with one, 62.7 with two and 44.6 for the row pipeline)
   if (F::id == FORM_F16 && (variant == 2 || variant == 4 || variant == 0)) {
     const int V = variant == 0 ? 4 : variant;

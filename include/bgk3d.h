@@ -27,8 +27,10 @@
  *    form stores scale*(f_q - w_q).
  *  - A context is not thread-safe. Its work runs in order on one CUDA stream
  *    owned by the context; calls that return host data synchronise it.
- *  - The library allocates all device memory it uses in bgk_create and on
- *    first use of a diagnostic, and frees it in bgk_destroy.
+ *  - The library allocates the device memory it uses in bgk_create and on
+ *    first use of a feature that needs more (diagnostics, spectrum, host
+ *    transfers, the adjoint and its state cache), keeps it for later calls
+ *    and frees it in bgk_destroy. bgk_diagnostics_noalloc allocates nothing.
  */
 #ifndef BGK3D_H
 #define BGK3D_H

@@ -355,3 +355,31 @@ def test_run_loop_writes_reference_files(bgk, tmp_path):
     assert abs(float(lines[0].split()[4]) - 1.0) < 1e-6
     assert len((tmp_path / "dissipation.dat").read_text().splitlines()[0].split()) == 4
     box.close()
+
+
+def test_tgv64_full_run_energy_and_dissipation_curves_vs_oracle(bgk, oracle_mod):
+    """Config C1 as a whole run: Taylor-Green 64^3, FP64, tau = 0.53
+    (svisc 0.01), U0 = 0.05, 500 steps, diagnostics every 10 steps. The GPU's
+    E(t) and dissipation curves match the oracle's to 1e-9 relative at every
+    record (the populations stay bit-exact, so the difference is only the
+    order of the compensated sums), and the populations still match bit for
+    bit at the end."""
+    n, svisc, u0 = 64, 0.01, 0.05
+    orc = oracle_mod.OracleLattice(n, n, n)
+    orc.init_tgv(u0, faithful=True)
+    box = bgk.BGK3D(n, svisc=svisc, u0=u0, icheck=10)
+    box.set_populations(orc.get_pops())
+    worst = 0.0
+    for it in range(1, 501):
+        orc.step(svisc, periodic=True)
+        box.col_MC(it)
+        d = box.diagnostic(it)
+        if d is None:
+            continue
+        dg = orc.diagno(False)
+        ds = orc.dissipation(svisc, u0, it, False)
+        for got, ref in ((d["ke_mean"], dg[4]), (d["tke_norm"], ds[1]), (d["diss"], ds[2]), (d["rho_mean"], dg[0])):
+            worst = max(worst, abs(got - ref) / abs(ref))
+    assert worst <= 1e-9, worst
+    assert same_bits(box.populations(), orc.get_pops())
+    box.close()

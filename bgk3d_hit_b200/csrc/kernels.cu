@@ -135,6 +135,77 @@ __device__ __forceinline__ void collide4_f16(uint2 (&Y)[Q], const StepK& K) {
   }
 }
 
+// The Smagorinsky collision of the FP16 form (lattice.cuh cell16_les) on four
+// cells packed in Y, one cell at a time so that no per-population array but
+// the cell's 19 inputs stays live: the Pi_neq sums are accumulated in the
+// order of cell16_les's expressions while the terms are formed, and the
+// equilibrium terms t_q are formed again for the output (the same operations,
+// so the same values). The output replaces the cell's half of Y.
+__device__ __forceinline__ void les16_cell(uint2 (&Y)[Q], int m, const StepK& k) {
+  float y[Q];
+#pragma unroll
+  for (int q = 0; q < Q; ++q) {
+    const float2 f = u2f2(m < 2 ? Y[q].x : Y[q].y);
+    y[q] = (m & 1) ? f.y : f.x;
+  }
+  const Mom16 M = moments16(y, k);
+  const float dr = M.dr;
+  auto tq = [&](int q) {
+    const float cu = cdotu(q, M);
+    const float P = __fmaf_rn(3.0f, cu, __fmaf_rn(__fmul_rn(4.5f, cu), cu, M.a));
+    return __fmaf_rn(dr, P, __fadd_rn(dr, P));
+  };
+  auto wf = [](int q) { return wclass(q) == 0 ? 1.0f / 3.0f : (wclass(q) == 1 ? 1.0f / 18.0f : 1.0f / 36.0f); };
+  float Pxx = 0.0f, Pyy = 0.0f, Pzz = 0.0f, Pxz = 0.0f, Pxy = 0.0f, Pyz = 0.0f;
+#pragma unroll
+  for (int q = 0; q < Q - 1; ++q) {
+    const float nn = __fsub_rn(__fmul_rn(y[q], k.inv), __fmul_rn(wf(q), tq(q)));
+    // Pxx = n0 + n1 + n2 + n3 + n4 + n9 + n10 + n11 + n12 + n13
+    if (q == 0) Pxx = nn;
+    else if (q <= 4 || (q >= 9 && q <= 13)) Pxx = Pxx + nn;
+    // Pyy = n0 + n2 + n6 + n7 + n8 + n9 + n11 + n15 + n16 + n17
+    if (q == 0) Pyy = nn;
+    else if (q == 2 || (q >= 6 && q <= 9) || q == 11 || q >= 15) Pyy = Pyy + nn;
+    // Pzz = n1 + n3 + n5 + n6 + n8 + n10 + n12 + n14 + n15 + n17
+    if (q == 1) Pzz = nn;
+    else if (q == 3 || q == 5 || q == 6 || q == 8 || q == 10 || q == 12 || q == 14 || q == 15 || q == 17) Pzz = Pzz + nn;
+    // Pxz = -n1 + n3 + n10 - n12
+    if (q == 1) Pxz = -nn;
+    else if (q == 3 || q == 10) Pxz = Pxz + nn;
+    else if (q == 12) Pxz = Pxz - nn;
+    // Pxy = -n0 + n2 + n9 - n11
+    if (q == 0) Pxy = -nn;
+    else if (q == 2 || q == 9) Pxy = Pxy + nn;
+    else if (q == 11) Pxy = Pxy - nn;
+    // Pyz = n6 - n8 + n15 - n17
+    if (q == 6) Pyz = nn;
+    else if (q == 15) Pyz = Pyz + nn;
+    else if (q == 8 || q == 17) Pyz = Pyz - nn;
+  }
+  float pt = __fmul_rn(Pxx, Pxx);
+  pt = __fmaf_rn(Pyy, Pyy, pt);
+  pt = __fmaf_rn(Pzz, Pzz, pt);
+  pt = __fmaf_rn(2.0f * Pxy, Pxy, pt);
+  pt = __fmaf_rn(2.0f * Pxz, Pxz, pt);
+  pt = __fmaf_rn(2.0f * Pyz, Pyz, pt);
+  const float tau = __fadd_rn(k.tauh_f, __fmul_rn(0.5f, __fsqrt_rn(__fmaf_rn(k.cs18_f, __fsqrt_rn(pt), k.tau2_f))));
+  const float om = __fdiv_rn(1.0f, tau);
+  const float om1 = __fsub_rn(1.0f, om);
+  const float oms = __fmul_rn(om, k.scale);
+#pragma unroll
+  for (int q = 0; q < Q; ++q) {
+    const unsigned short h =
+        __half_as_ushort(__float2half_rn(__fmaf_rn(__fmul_rn(oms, wf(q)), tq(q), __fmul_rn(om1, y[q]))));
+    unsigned& word = m < 2 ? Y[q].x : Y[q].y;
+    word = (m & 1) ? ((word & 0xffffu) | ((unsigned)h << 16)) : ((word & 0xffff0000u) | h);
+  }
+}
+
+__device__ __forceinline__ void collide4_f16_les(uint2 (&Y)[Q], const StepK& K) {
+#pragma unroll
+  for (int m = 0; m < 4; ++m) les16_cell(Y, m, K);
+}
+
 // Lanes that exchange x-neighbours in the four-cells-per-thread FP16 kernels:
 // a row of nx cells is tpr = nx/4 consecutive threads. Rows shorter than a warp
 // wrap inside it; rows of one or more warps wrap through global memory at the
@@ -209,6 +280,7 @@ __device__ __forceinline__ void shift_out(uint2 Y, int cx, __half* p, int i0, in
   }
 }
 
+template <bool LES>
 __global__ void __launch_bounds__(256, 3) k_two_f16v(Pops<const __half> src, Pops<__half> dst, Geo g, StepK K,
                                                   int log_tpr) {
   const int tpr = 1 << log_tpr;
@@ -254,7 +326,8 @@ __global__ void __launch_bounds__(256, 3) k_two_f16v(Pops<const __half> src, Pop
       Y[q].y = __byte_perm(A.y, next, 0x5432);
     }
   }
-  collide4_f16(Y, K);
+  if constexpr (LES) collide4_f16_les(Y, K);
+  else collide4_f16(Y, K);
   const int o = i0 + g.sx * (j + g.ny * k);
 #pragma unroll
   for (int q = 0; q < Q; ++q) *reinterpret_cast<uint2*>(dst.p[q] + o) = Y[q];
@@ -394,7 +467,7 @@ __global__ void __launch_bounds__(256, 5) k_aa_f16_odd(Pops<__half> a, Geo g, St
 // that measured 69.5 GLUPS for the pair of steps, against 63.4 with both
 // capped at 3 (282 spilled bytes in the odd step) and 58 for one cell per
 // thread.
-template <bool ODD>
+template <bool ODD, bool LES>
 __global__ void __launch_bounds__(256, ODD ? 2 : 3) k_aa_f16v(Pops<__half> a, Geo g, StepK K, int log_tpr) {
   const int tpr = 1 << log_tpr;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -422,7 +495,8 @@ __global__ void __launch_bounds__(256, ODD ? 2 : 3) k_aa_f16v(Pops<__half> a, Ge
       Y[q] = shift_in(__ldg(reinterpret_cast<const uint2*>(p + i0)), cxq(q), p, i_prev, i_next, xl);
     }
   }
-  collide4_f16(Y, K);
+  if constexpr (LES) collide4_f16_les(Y, K);
+  else collide4_f16(Y, K);
 #pragma unroll
   for (int q = 0; q < Q; ++q) {
     if (!ODD) *reinterpret_cast<uint2*>(a.p[oppq(q)] + row(0, 0) + i0) = Y[q];
@@ -918,8 +992,16 @@ static cudaError_t two_impl(const Lattice& s, const Lattice& d, const StepK& K, 
   Pops<S> pd = pops_of<S>(d);
   pd.p[Q - 1] = (S*)s.p[Q - 1];  // pop 19 in place (SRC/col_MC.F90:351)
   Shape sh = cell_shape(s.g);
-  if (K.les) {  // the Smagorinsky collision runs on the one cell per thread kernel
-    k_two<F, true><<<sh.grid, sh.block, 0, st>>>(ps, pd, s.g, K);
+  if (K.les) {  // the Smagorinsky collision: one cell per thread, FP16 four where the box fits
+    const int lt = F::id == FORM_F16 && (variant == 0 || variant == 4) ? f16v_log_tpr(s.g, 4) : -1;
+    if (lt >= 0) {
+      Pops<__half> ph = pops_of<__half>(d);
+      ph.p[Q - 1] = (__half*)s.p[Q - 1];
+      dim3 grid((unsigned)((((long long)s.g.ny << lt) + 255) / 256), s.g.nz);
+      k_two_f16v<true><<<grid, 256, 0, st>>>(pops_of<const __half>(s), ph, s.g, K, lt);
+    } else {
+      k_two<F, true><<<sh.grid, sh.block, 0, st>>>(ps, pd, s.g, K);
+    }
     return cudaGetLastError();
   }
   if (variant == 8) {
@@ -939,7 +1021,7 @@ static cudaError_t two_impl(const Lattice& s, const Lattice& d, const StepK& K, 
       dim3 grid((unsigned)((threads + 255) / 256), s.g.nz);
       Pops<__half> ph = pops_of<__half>(d);
       ph.p[Q - 1] = (__half*)s.p[Q - 1];
-      if (V == 4) k_two_f16v<<<grid, 256, 0, st>>>(pops_of<const __half>(s), ph, s.g, K, lt);
+      if (V == 4) k_two_f16v<false><<<grid, 256, 0, st>>>(pops_of<const __half>(s), ph, s.g, K, lt);
       else k_two_f16v2<<<grid, 256, 0, st>>>(pops_of<const __half>(s), ph, s.g, K, lt);
       return cudaGetLastError();
     }
@@ -977,9 +1059,17 @@ template <class F>
 static cudaError_t aa_impl(const Lattice& a, int odd, const StepK& K, int variant, cudaStream_t st) {
   using S = typename F::S;
   Shape sh = cell_shape(a.g);
+  const int lt4 = F::id == FORM_F16 && (variant == 0 || variant == 4) ? f16v_log_tpr(a.g, 4) : -1;
   if (K.les) {
-    if (odd) k_aa<F, true, true><<<sh.grid, sh.block, 0, st>>>(pops_of<S>(a), a.g, K);
-    else k_aa<F, false, true><<<sh.grid, sh.block, 0, st>>>(pops_of<S>(a), a.g, K);
+    if (lt4 >= 0) {
+      dim3 grid((unsigned)((((long long)a.g.ny << lt4) + 255) / 256), a.g.nz);
+      if (odd) k_aa_f16v<true, true><<<grid, 256, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
+      else k_aa_f16v<false, true><<<grid, 256, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
+    } else if (odd) {
+      k_aa<F, true, true><<<sh.grid, sh.block, 0, st>>>(pops_of<S>(a), a.g, K);
+    } else {
+      k_aa<F, false, true><<<sh.grid, sh.block, 0, st>>>(pops_of<S>(a), a.g, K);
+    }
     return cudaGetLastError();
   }
   if (variant == 8) {
@@ -988,14 +1078,11 @@ static cudaError_t aa_impl(const Lattice& a, int odd, const StepK& K, int varian
     if (e != cudaSuccess || launched) return e;
   }
   // FP16: four cells per thread where the box fits it (automatic or 4)
-  if (F::id == FORM_F16 && (variant == 0 || variant == 4)) {
-    const int lt = f16v_log_tpr(a.g, 4);
-    if (lt >= 0) {
-      dim3 grid((unsigned)((((long long)a.g.ny << lt) + 255) / 256), a.g.nz);
-      if (odd) k_aa_f16v<true><<<grid, 256, 0, st>>>(pops_of<__half>(a), a.g, K, lt);
-      else k_aa_f16v<false><<<grid, 256, 0, st>>>(pops_of<__half>(a), a.g, K, lt);
-      return cudaGetLastError();
-    }
+  if (lt4 >= 0) {
+    dim3 grid((unsigned)((((long long)a.g.ny << lt4) + 255) / 256), a.g.nz);
+    if (odd) k_aa_f16v<true, false><<<grid, 256, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
+    else k_aa_f16v<false, false><<<grid, 256, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
+    return cudaGetLastError();
   }
   if (odd && F::id == FORM_F16)
     k_aa_f16_odd<<<sh.grid, sh.block, 0, st>>>(pops_of<__half>(a), a.g, K);

@@ -3,8 +3,9 @@ reference's -DLES block of SRC/col_MC.F90:221-309, through the C-ABI.
 
 Tolerance: bit-exact against the oracle in all three forms and both schemes
 (the kernels round every operation, square roots included, as the oracle
-does); kernel choices 2/4/8 fall back to the one cell per thread kernels and
-give the same bits."""
+does), with the FP16 four-cells-per-thread kernels where a box fits them
+(rows inside a warp, one and two warps per row); kernel choices 2/8 fall back
+to the one cell per thread kernels and give the same bits."""
 import numpy as np
 import pytest
 
@@ -34,7 +35,7 @@ def _pair(bgk, O, shape, form, scheme, cs, svisc, init, kernel=0):
 @pytest.mark.parametrize("form", ["fp64", "fp32", "fp16"])
 @pytest.mark.parametrize("scheme", ["two_lattice", "aa"])
 @pytest.mark.parametrize("case", [("tgv", (33, 20, 7), 0.17), ("hit", (16, 16, 16), 0.17),
-                                  ("hit", (16, 16, 16), 1.0)])
+                                  ("hit", (16, 16, 16), 1.0), ("tgv", (128, 8, 6), 0.17), ("tgv", (256, 4, 4), 1.0)])
 def test_les_bitexact_vs_oracle(bgk, oracle_mod, form, scheme, case):
     init, shape, cs = case
     orc, box = _pair(bgk, oracle_mod, shape, form, scheme, cs, 1e-4, init)

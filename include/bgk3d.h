@@ -96,7 +96,8 @@ typedef struct {
                           per cell Ptotal = |Pi_neq|, Ts = 1/(2 omega) +
                           sqrt(18 cteS^2 Ptotal + (1/omega)^2)/2, relaxation with 1/Ts.
                           0 (default) = plain BGK. The LES collision runs on the one
-                          cell per thread kernels (kernel 2/4/8 fall back to them);
+                          cell per thread kernels, and in FP16 on the four cells per
+                          thread kernels where the box fits (kernel 2/8 fall back);
                           bgk_adjoint and bgk_tangent reject it. */
   int proc_z;          /* number of z-slabs the box is split into (the reference's
                           proc_z, SRC/input.F90:41; proc_x = proc_y = 1). 1 (default):

@@ -89,10 +89,11 @@ __global__ void __launch_bounds__(256) k_two(Pops<const typename F::S> src, Pops
 // neighbouring lane (warp shuffle); across warp boundaries (tpr > 32) lanes 0
 // and 31 load it. Each cell's arithmetic is F16::cell's (moments16, pair16,
 // rest16). The collision runs on two cells at a time, their outputs replacing
-// their inputs in the packed registers, and the kernel is capped at 3 blocks
-// per SM (80 registers, a few spilled bytes): on B200 at 256^3 that measured
-// 76.6 GLUPS, against 64.5 for all four cells at once at 2 blocks per SM and
-// 58.4 at 4 blocks per SM (heavy spills).
+// their inputs in the packed registers, and the kernel runs 128-thread blocks
+// capped at 80 registers (6 blocks per SM, a few spilled bytes): on B200 at
+// 256^3 that measured 78.4-79.4 GLUPS, against 76.6 with 256-thread blocks at
+// the same cap, 64.5 for all four cells at once at 2 blocks per SM and 58.4
+// at 64 registers (heavy spills).
 __device__ __forceinline__ unsigned short ldg_u16(const __half* p) {
   return __ldg(reinterpret_cast<const unsigned short*>(p));
 }
@@ -281,7 +282,7 @@ __device__ __forceinline__ void shift_out(uint2 Y, int cx, __half* p, int i0, in
 }
 
 template <bool LES>
-__global__ void __launch_bounds__(256, 3) k_two_f16v(Pops<const __half> src, Pops<__half> dst, Geo g, StepK K,
+__global__ void __launch_bounds__(128, 6) k_two_f16v(Pops<const __half> src, Pops<__half> dst, Geo g, StepK K,
                                                   int log_tpr) {
   const int tpr = 1 << log_tpr;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -461,14 +462,14 @@ __global__ void __launch_bounds__(256, 5) k_aa_f16_odd(Pops<__half> a, Geo g, St
 // the store side. Every (location, slot) pair is still read and written by the
 // thread of the cell that owns it in the one-cell-per-thread kernel, or by a
 // lane of the same warp after a shuffle that orders it behind the owner's
-// loads, so the in-place update stays race-free. The even step is capped at 3
-// blocks per SM like k_two_f16v; the odd step, whose shifted stores need more
-// registers, runs uncapped at 2 (128 registers, no spills): on B200 at 256^3
-// that measured 69.5 GLUPS for the pair of steps, against 63.4 with both
-// capped at 3 (282 spilled bytes in the odd step) and 58 for one cell per
-// thread.
+// loads, so the in-place update stays race-free. 128-thread blocks; the even
+// step is capped at 80 registers like k_two_f16v, the odd step, whose shifted
+// accesses need more registers, at 128 (no spills): on B200 at 256^3 that
+// measured 71.0 GLUPS for the pair of steps, against 69.5 with 256-thread
+// blocks, 63.4 with the odd step also capped at 80 registers (282 spilled
+// bytes) and 58 for one cell per thread.
 template <bool ODD, bool LES>
-__global__ void __launch_bounds__(256, ODD ? 2 : 3) k_aa_f16v(Pops<__half> a, Geo g, StepK K, int log_tpr) {
+__global__ void __launch_bounds__(128, ODD ? 4 : 6) k_aa_f16v(Pops<__half> a, Geo g, StepK K, int log_tpr) {
   const int tpr = 1 << log_tpr;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = t >> log_tpr, pos = t & (tpr - 1);
@@ -997,8 +998,8 @@ static cudaError_t two_impl(const Lattice& s, const Lattice& d, const StepK& K, 
     if (lt >= 0) {
       Pops<__half> ph = pops_of<__half>(d);
       ph.p[Q - 1] = (__half*)s.p[Q - 1];
-      dim3 grid((unsigned)((((long long)s.g.ny << lt) + 255) / 256), s.g.nz);
-      k_two_f16v<true><<<grid, 256, 0, st>>>(pops_of<const __half>(s), ph, s.g, K, lt);
+      dim3 grid((unsigned)((((long long)s.g.ny << lt) + 127) / 128), s.g.nz);
+      k_two_f16v<true><<<grid, 128, 0, st>>>(pops_of<const __half>(s), ph, s.g, K, lt);
     } else {
       k_two<F, true><<<sh.grid, sh.block, 0, st>>>(ps, pd, s.g, K);
     }
@@ -1018,10 +1019,10 @@ static cudaError_t two_impl(const Lattice& s, const Lattice& d, const StepK& K, 
     const int lt = f16v_log_tpr(s.g, V);
     if (lt >= 0) {
       const long long threads = (long long)s.g.ny << lt;
-      dim3 grid((unsigned)((threads + 255) / 256), s.g.nz);
+      dim3 grid((unsigned)((threads + (V == 4 ? 127 : 255)) / (V == 4 ? 128 : 256)), s.g.nz);
       Pops<__half> ph = pops_of<__half>(d);
       ph.p[Q - 1] = (__half*)s.p[Q - 1];
-      if (V == 4) k_two_f16v<false><<<grid, 256, 0, st>>>(pops_of<const __half>(s), ph, s.g, K, lt);
+      if (V == 4) k_two_f16v<false><<<grid, 128, 0, st>>>(pops_of<const __half>(s), ph, s.g, K, lt);
       else k_two_f16v2<<<grid, 256, 0, st>>>(pops_of<const __half>(s), ph, s.g, K, lt);
       return cudaGetLastError();
     }
@@ -1062,9 +1063,9 @@ static cudaError_t aa_impl(const Lattice& a, int odd, const StepK& K, int varian
   const int lt4 = F::id == FORM_F16 && (variant == 0 || variant == 4) ? f16v_log_tpr(a.g, 4) : -1;
   if (K.les) {
     if (lt4 >= 0) {
-      dim3 grid((unsigned)((((long long)a.g.ny << lt4) + 255) / 256), a.g.nz);
-      if (odd) k_aa_f16v<true, true><<<grid, 256, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
-      else k_aa_f16v<false, true><<<grid, 256, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
+      dim3 grid((unsigned)((((long long)a.g.ny << lt4) + 127) / 128), a.g.nz);
+      if (odd) k_aa_f16v<true, true><<<grid, 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
+      else k_aa_f16v<false, true><<<grid, 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
     } else if (odd) {
       k_aa<F, true, true><<<sh.grid, sh.block, 0, st>>>(pops_of<S>(a), a.g, K);
     } else {
@@ -1079,9 +1080,9 @@ static cudaError_t aa_impl(const Lattice& a, int odd, const StepK& K, int varian
   }
   // FP16: four cells per thread where the box fits it (automatic or 4)
   if (lt4 >= 0) {
-    dim3 grid((unsigned)((((long long)a.g.ny << lt4) + 255) / 256), a.g.nz);
-    if (odd) k_aa_f16v<true, false><<<grid, 256, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
-    else k_aa_f16v<false, false><<<grid, 256, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
+    dim3 grid((unsigned)((((long long)a.g.ny << lt4) + 127) / 128), a.g.nz);
+    if (odd) k_aa_f16v<true, false><<<grid, 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
+    else k_aa_f16v<false, false><<<grid, 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
     return cudaGetLastError();
   }
   if (odd && F::id == FORM_F16)

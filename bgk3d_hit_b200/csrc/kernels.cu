@@ -283,11 +283,11 @@ __device__ __forceinline__ void shift_out(uint2 Y, int cx, __half* p, int i0, in
 
 template <bool LES>
 __global__ void __launch_bounds__(128, 6) k_two_f16v(Pops<const __half> src, Pops<__half> dst, Geo g, StepK K,
-                                                  int log_tpr) {
+                                                  int log_tpr, int k0) {
   const int tpr = 1 << log_tpr;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = t >> log_tpr, pos = t & (tpr - 1);
-  const int k = blockIdx.y;
+  const int k = blockIdx.y + k0;  // planes k0 .. k0 + gridDim.y - 1
   if (j >= g.ny) return;  // whole warps: ny*tpr is a multiple of 32
   const int lane = threadIdx.x & 31;
   const int i0 = pos * 4;
@@ -999,7 +999,7 @@ static cudaError_t two_impl(const Lattice& s, const Lattice& d, const StepK& K, 
       Pops<__half> ph = pops_of<__half>(d);
       ph.p[Q - 1] = (__half*)s.p[Q - 1];
       dim3 grid((unsigned)((((long long)s.g.ny << lt) + 127) / 128), s.g.nz);
-      k_two_f16v<true><<<grid, 128, 0, st>>>(pops_of<const __half>(s), ph, s.g, K, lt);
+      k_two_f16v<true><<<grid, 128, 0, st>>>(pops_of<const __half>(s), ph, s.g, K, lt, 0);
     } else {
       k_two<F, true><<<sh.grid, sh.block, 0, st>>>(ps, pd, s.g, K);
     }
@@ -1022,7 +1022,7 @@ static cudaError_t two_impl(const Lattice& s, const Lattice& d, const StepK& K, 
       dim3 grid((unsigned)((threads + (V == 4 ? 127 : 255)) / (V == 4 ? 128 : 256)), s.g.nz);
       Pops<__half> ph = pops_of<__half>(d);
       ph.p[Q - 1] = (__half*)s.p[Q - 1];
-      if (V == 4) k_two_f16v<false><<<grid, 128, 0, st>>>(pops_of<const __half>(s), ph, s.g, K, lt);
+      if (V == 4) k_two_f16v<false><<<grid, 128, 0, st>>>(pops_of<const __half>(s), ph, s.g, K, lt, 0);
       else k_two_f16v2<<<grid, 256, 0, st>>>(pops_of<const __half>(s), ph, s.g, K, lt);
       return cudaGetLastError();
     }
@@ -1238,9 +1238,21 @@ static cudaError_t slab_impl(const Lattice& s, const Lattice& d, const StepK& K,
   if (K.les) k_slab<F, true, true><<<ge, sh.block, 0, st>>>(ps, pd, s.g, K, h);
   else k_slab<F, false, true><<<ge, sh.block, 0, st>>>(ps, pd, s.g, K, h);
   if (s.g.nz > 2) {
-    const dim3 gi(sh.grid.x, sh.grid.y, s.g.nz - 2);
-    if (K.les) k_slab<F, true, false><<<gi, sh.block, 0, st>>>(ps, pd, s.g, K, h);
-    else k_slab<F, false, false><<<gi, sh.block, 0, st>>>(ps, pd, s.g, K, h);
+    // FP16: the interior planes on the four-cells-per-thread kernel where the
+    // rows fit it (planes 1 .. nz-2 pull only inside the slab, so its z wrap
+    // never applies)
+    const int lt = F::id == FORM_F16 ? f16v_log_tpr(s.g, 4) : -1;
+    if (lt >= 0) {
+      Pops<__half> ph = pops_of<__half>(d);
+      ph.p[Q - 1] = (__half*)s.p[Q - 1];
+      const dim3 gv((unsigned)((((long long)s.g.ny << lt) + 127) / 128), s.g.nz - 2);
+      if (K.les) k_two_f16v<true><<<gv, 128, 0, st>>>(pops_of<const __half>(s), ph, s.g, K, lt, 1);
+      else k_two_f16v<false><<<gv, 128, 0, st>>>(pops_of<const __half>(s), ph, s.g, K, lt, 1);
+    } else {
+      const dim3 gi(sh.grid.x, sh.grid.y, s.g.nz - 2);
+      if (K.les) k_slab<F, true, false><<<gi, sh.block, 0, st>>>(ps, pd, s.g, K, h);
+      else k_slab<F, false, false><<<gi, sh.block, 0, st>>>(ps, pd, s.g, K, h);
+    }
   }
   return cudaGetLastError();
 }

@@ -29,10 +29,11 @@ def _kw(form, **kw):
 @pytest.mark.parametrize("form", ["fp64", "fp32", "fp16"])
 @pytest.mark.parametrize("proc_z", [2, 3, 4])
 @pytest.mark.parametrize("les_cs", [0.0, 0.17])
-def test_local_slabs_bitexact_vs_whole_box(bgk, form, proc_z, les_cs):
+@pytest.mark.parametrize("nx", [20, 32])  # 32: FP16 interior planes on the four-cells-per-thread kernel
+def test_local_slabs_bitexact_vs_whole_box(bgk, form, proc_z, les_cs, nx):
     from bgk3d_hit_b200.slabs import LocalSlabs
 
-    shape = (20, 12, 24)
+    shape = (nx, 12, 24)
     box = bgk.BGK3D(*shape, **_kw(form, les_cs=les_cs))
     box.init()
     sl = LocalSlabs(*shape, proc_z, **_kw(form, les_cs=les_cs))

@@ -52,6 +52,9 @@ struct bgk_ctx {
   int form = 0, scheme = 0;
   cudaStream_t st = nullptr;
   cudaEvent_t mark = nullptr;  // bgk_record_event / bgk_wait_event
+  // z-slab: second stream for the interior planes and its fork / join events
+  cudaStream_t st_in = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   Geo g{};
   size_t es = 8;
   void* memA = nullptr;
@@ -453,6 +456,10 @@ int bgk_create(const bgk_params* p, bgk_ctx** out) {
     c->halo_bytes = (size_t)(2 * 2 * NZF) * (size_t)c->plane_elems * c->es;
     rc = dev_alloc(c, &c->halo_mem, c->halo_bytes, "ghost planes");
     if (rc) return fail(rc);
+    e = cudaStreamCreateWithFlags(&c->st_in, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming);
+    if (e != cudaSuccess) return fail(cuda_fail(e, "slab stream"));
     e = cudaMemsetAsync(c->halo_mem, 0, c->halo_bytes, c->st);
     if (e != cudaSuccess) return fail(cuda_fail(e, "cudaMemset"));
   }
@@ -464,6 +471,7 @@ int bgk_create(const bgk_params* p, bgk_ctx** out) {
 int bgk_destroy(bgk_ctx* c) {
   if (!c) return BGK_OK;
   cudaSetDevice(c->p.device);
+  if (c->st_in) cudaStreamSynchronize(c->st_in);
   if (c->st) cudaStreamSynchronize(c->st);
   if (c->plan_ok) cufftDestroy(c->plan);
   cudaFree(c->memA);
@@ -485,6 +493,9 @@ int bgk_destroy(bgk_ctx* c) {
   cudaFree(c->adj_tot);
   if (c->h_tot) cudaFreeHost(c->h_tot);
   if (c->mark) cudaEventDestroy(c->mark);
+  if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+  if (c->ev_join) cudaEventDestroy(c->ev_join);
+  if (c->st_in) cudaStreamDestroy(c->st_in);
   if (c->st) cudaStreamDestroy(c->st);
   delete c;
   return BGK_OK;
@@ -578,8 +589,15 @@ int bgk_col_mc(bgk_ctx* c, int itime) {
     return BGK_ERR_STATE;
   }
   if (c->slab) {
+    // boundary planes on the context's stream, interior planes side by side on
+    // the second one; the join puts everything later on the context's stream
+    // behind both
     const SlabLinks l = slab_links(c, (int)(c->step & 1), (int)((c->step + 1) & 1));
-    CK(launch_slab(c->A, c->B, l, c->omega, c->scale, c->p.les_cs, c->st));
+    CK(cudaEventRecord(c->ev_fork, c->st));
+    CK(cudaStreamWaitEvent(c->st_in, c->ev_fork, 0));
+    CK(launch_slab(c->A, c->B, l, c->omega, c->scale, c->p.les_cs, c->st, c->st_in));
+    CK(cudaEventRecord(c->ev_join, c->st_in));
+    CK(cudaStreamWaitEvent(c->st, c->ev_join, 0));
     if (c->g.nz > 2) c->launches++;  // edge planes and interior are two launches
   } else if (c->scheme == BGK_TWO_LATTICE) {
     CK(launch_two_lattice(c->A, c->B, c->omega, c->scale, c->p.les_cs, c->p.kernel, c->st));

@@ -1226,14 +1226,16 @@ cudaError_t launch_diag(const Lattice& a, int lay, double svisc, double omega, d
 
 template <class F>
 static cudaError_t slab_impl(const Lattice& s, const Lattice& d, const StepK& K, const SlabLinks& l,
-                             cudaStream_t st) {
+                             cudaStream_t st, cudaStream_t st_in) {
   using S = typename F::S;
   Pops<const S> ps = pops_of<const S>(s);
   Pops<S> pd = pops_of<S>(d);
   pd.p[Q - 1] = (S*)s.p[Q - 1];  // pop 19 in place (SRC/col_MC.F90:351)
   const Shape sh = cell_shape(s.g);
   const Halo<S> h = halo_of<S>(&l);
-  // planes 0 and nz-1 (one plane when nz = 1), then the interior
+  // planes 0 and nz-1 (one plane when nz = 1) on st, the interior on st_in:
+  // the two read only the source lattice and write disjoint planes, so they
+  // may run side by side
   const dim3 ge(sh.grid.x, sh.grid.y, s.g.nz > 1 ? 2 : 1);
   if (K.les) k_slab<F, true, true><<<ge, sh.block, 0, st>>>(ps, pd, s.g, K, h);
   else k_slab<F, false, true><<<ge, sh.block, 0, st>>>(ps, pd, s.g, K, h);
@@ -1246,24 +1248,24 @@ static cudaError_t slab_impl(const Lattice& s, const Lattice& d, const StepK& K,
       Pops<__half> ph = pops_of<__half>(d);
       ph.p[Q - 1] = (__half*)s.p[Q - 1];
       const dim3 gv((unsigned)((((long long)s.g.ny << lt) + 127) / 128), s.g.nz - 2);
-      if (K.les) k_two_f16v<true><<<gv, 128, 0, st>>>(pops_of<const __half>(s), ph, s.g, K, lt, 1);
-      else k_two_f16v<false><<<gv, 128, 0, st>>>(pops_of<const __half>(s), ph, s.g, K, lt, 1);
+      if (K.les) k_two_f16v<true><<<gv, 128, 0, st_in>>>(pops_of<const __half>(s), ph, s.g, K, lt, 1);
+      else k_two_f16v<false><<<gv, 128, 0, st_in>>>(pops_of<const __half>(s), ph, s.g, K, lt, 1);
     } else {
       const dim3 gi(sh.grid.x, sh.grid.y, s.g.nz - 2);
-      if (K.les) k_slab<F, true, false><<<gi, sh.block, 0, st>>>(ps, pd, s.g, K, h);
-      else k_slab<F, false, false><<<gi, sh.block, 0, st>>>(ps, pd, s.g, K, h);
+      if (K.les) k_slab<F, true, false><<<gi, sh.block, 0, st_in>>>(ps, pd, s.g, K, h);
+      else k_slab<F, false, false><<<gi, sh.block, 0, st_in>>>(ps, pd, s.g, K, h);
     }
   }
   return cudaGetLastError();
 }
 
 cudaError_t launch_slab(const Lattice& src, const Lattice& dst, const SlabLinks& links, double omega, double scale,
-                        double les_cs, cudaStream_t st) {
+                        double les_cs, cudaStream_t st, cudaStream_t st_interior) {
   const StepK K = make_stepk(src.form, omega, scale, les_cs);
   switch (src.form) {
-    case FORM_F64: return slab_impl<F64>(src, dst, K, links, st);
-    case FORM_F32: return slab_impl<F32>(src, dst, K, links, st);
-    case FORM_F16: return slab_impl<F16>(src, dst, K, links, st);
+    case FORM_F64: return slab_impl<F64>(src, dst, K, links, st, st_interior);
+    case FORM_F32: return slab_impl<F32>(src, dst, K, links, st, st_interior);
+    case FORM_F16: return slab_impl<F16>(src, dst, K, links, st, st_interior);
   }
   return cudaErrorInvalidValue;
 }

@@ -103,10 +103,11 @@ cudaError_t launch_diag(const Lattice& a, int lay, double svisc, double omega, d
 
 // z-slab two-lattice step (src -> dst, pop 19 in place) reading the ghost
 // planes links.in_* and storing the outgoing boundary populations into
-// links.up / links.dn; and the fill of links.up / links.dn from the current
-// state alone.
+// links.up / links.dn: the boundary planes on st, the interior planes on
+// st_interior (the caller orders the two streams); and the fill of
+// links.up / links.dn from the current state alone.
 cudaError_t launch_slab(const Lattice& src, const Lattice& dst, const SlabLinks& links, double omega, double scale,
-                        double les_cs, cudaStream_t st);
+                        double les_cs, cudaStream_t st, cudaStream_t st_interior);
 cudaError_t launch_halo_prime(const Lattice& a, const SlabLinks& links, cudaStream_t st);
 cudaError_t launch_enstrophy(const Lattice& a, const void* vel, double* partials, cudaStream_t st);
 // Sums DIAG_BLOCKS partials into ND totals (fixed order, compensated).

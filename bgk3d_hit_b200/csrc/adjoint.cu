@@ -90,14 +90,14 @@ __global__ void __launch_bounds__(DIAG_THREADS) k_adj_terminal(Pops<const typena
 // So no population array stays live across the cell. lam is read again from
 // cache for the output. rho and u are formed in the form's arithmetic R, the
 // moment sums and A, B, G in double. Each block adds its dL/domega
-// contribution (warp shuffles, then the eight warp sums in order) into its
+// contribution (warp shuffles, then the four warp sums in order) into its
 // own compensated pair acc[2*block].
 template <class F>
-__global__ void __launch_bounds__(256, 2) k_adj_step(Pops<const typename F::S> ft, Pops<const typename F::S> lin,
+__global__ void __launch_bounds__(128, 4) k_adj_step(Pops<const typename F::S> ft, Pops<const typename F::S> lin,
                                                      Pops<typename F::S> lout, Geo g, typename F::R omega,
                                                      double* acc) {
   using S = typename F::S; using R = typename F::R;
-  __shared__ double wsum[8];
+  __shared__ double wsum[4];
   double dw = 0.0;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
@@ -165,7 +165,7 @@ __global__ void __launch_bounds__(256, 2) k_adj_step(Pops<const typename F::S> f
   __syncthreads();
   if (t == 0) {
     double s = 0.0;
-    for (int w = 0; w < 8; ++w) s += wsum[w];
+    for (int w = 0; w < 4; ++w) s += wsum[w];
     const long long b = blockIdx.x + (long long)gridDim.x * (blockIdx.y + (long long)gridDim.y * blockIdx.z);
     KS a2{acc[2 * b], acc[2 * b + 1]};
     kadd(a2, s);
@@ -302,10 +302,10 @@ __global__ void __launch_bounds__(DIAG_THREADS) k_acc_total(const double* __rest
   if (threadIdx.x == 0) *total = __dadd_rn(r.s, r.c);
 }
 
-// Launch shape of the per-cell kernels (x rows in blockDim.x, 256 threads).
+// Launch shape of the adjoint step (x rows in blockDim.x, 128 threads).
 void adj_shape(const Geo& g, dim3* grid, dim3* block) {
   const int tx = g.nx >= 128 ? 128 : ((g.nx + 31) / 32) * 32;
-  const int ty = 256 / tx;
+  const int ty = 128 / tx;
   *block = dim3(tx, ty, 1);
   *grid = dim3((g.nx + tx - 1) / tx, (g.ny + ty - 1) / ty, g.nz);
 }

@@ -319,7 +319,7 @@ def run_ours(a):
     if rank == 0 and ws == 1 and not a.no_cpu:
         try:
             cpu = cpu_baseline(a, a.cpu_seconds)
-        except Exception as ex:  # the checker is optional for the GPU number
+        except Exception as ex:  # the CPU baseline is optional for the GPU number
             cpu = {"value": None, "unit": "GLUPS", "cores": os.cpu_count(), "kind": "port", "sample": f"failed: {ex}"}
 
     if rank == 0:

@@ -19,7 +19,7 @@ Loss = 0.5 mean |u(T) - u_tgt|^2. Reports, as one JSON object:
 - vs_fp64 (FP32 storage only): the relative L2 difference between the FP32
   gradient and the FP64 adjoint gradient of the same problem (central
   differences of an FP32 loss over 1000 steps are dominated by its rounding,
-  so the FP32 gradient is judged against FP64 instead).
+  so the FP32 gradient is compared with FP64 instead).
 """
 from __future__ import annotations
 

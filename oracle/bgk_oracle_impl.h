@@ -1,9 +1,9 @@
 /*
  * CPU restatement of the BGK3D_HIT time-step hot path (TEST INFRASTRUCTURE).
  *
- * This file is the oracle: tests, the smoke check and the CPU-baseline leg of
- * the benchmark use it as the checker. Nothing in the product library links,
- * loads or calls it.
+ * This file is the oracle: tests and the smoke check use it to check results,
+ * the benchmark's CPU legs as the timed CPU baseline. Nothing in the product
+ * library links, loads or calls it.
  *
  * Parity unpinned: the reference ships no tests, golden vectors or fixtures,
  * and its Fortran/MPI build cannot be compiled in this environment (no Fortran

@@ -2,7 +2,7 @@
 
 The oracle restates the reference's Fortran hot path in C (``bgk_oracle.c``).
 Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
-``bench.py`` import this module, and only as the checker / timed CPU baseline.
+``bench.py`` import this module, and only to check results or as the timed CPU baseline.
 The product library never loads it.
 
 Parity unpinned: the reference ships no golden vectors and cannot be compiled

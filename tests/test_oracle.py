@@ -1,4 +1,4 @@
-"""CPU tests of the oracle (the checker): internal consistency, exact
+"""CPU tests of the oracle: internal consistency, exact
 arithmetic of a single cell, the reference's halo semantics, physics
 known answers and the committed golden fixtures."""
 from fractions import Fraction as Fr

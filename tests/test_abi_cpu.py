@@ -163,3 +163,22 @@ def test_driver_builds_and_rejects_bad_input(tmp_path):
     assert r.returncode == 2 and "one box per process" in r.stderr
     r = subprocess.run([exe, "--help"], capture_output=True, text=True)
     assert r.returncode == 0 and "usage" in r.stdout
+
+
+def test_bench_reference_arm_line_on_cpu():
+    """bench.py --impl reference times the oracle's restatement of the
+    reference on the host and prints one JSON line with the contract's keys
+    (it needs no GPU)."""
+    import json
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--impl", "reference", "--size", "16",
+                        "--steps", "3", "--warmup", "1"], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    line = json.loads(r.stdout.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and line["unit"] == "GLUPS" and line["value"] > 0
+    for k in ("metric", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better", "config", "cpu_baseline", "e2e"):
+        assert k in line, k
+    assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["cores"] >= 1
+    assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["value"] == line["value"]

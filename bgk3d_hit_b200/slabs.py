@@ -45,6 +45,18 @@ def slab_range(lz: int, proc_z: int, coord_z: int) -> tuple[int, int]:
     return coord_z * n, n
 
 
+def split_z(a, global_shape, proc_z: int) -> list:
+    """A (lz, ly, lx) global array (any layout numpy can reshape to it) as
+    the proc_z slabs' views, slab r holding planes slab_range(lz, proc_z, r)."""
+    lx, ly, lz = global_shape
+    a = np.asarray(a).reshape(lz, ly, lx)
+    out = []
+    for r in range(proc_z):
+        z0, n = slab_range(lz, proc_z, r)
+        out.append(a[z0:z0 + n])
+    return out
+
+
 def neighbours(coord_z: int, proc_z: int) -> tuple[int, int]:
     """Slabs below and above, periodic in z."""
     return (coord_z - 1) % proc_z, (coord_z + 1) % proc_z
@@ -137,14 +149,7 @@ class LocalSlabs:
         self.barrier()
 
     def _split(self, a):
-        """(lz, ly, lx) global array -> per-slab views."""
-        lx, ly, lz = self.global_shape
-        a = np.asarray(a).reshape(lz, ly, lx)
-        out = []
-        for r in range(self.proc_z):
-            z0, n = slab_range(lz, self.proc_z, r)
-            out.append(a[z0:z0 + n])
-        return out
+        return split_z(a, self.global_shape, self.proc_z)
 
     def init(self):
         for s in self.slabs:

@@ -21,6 +21,17 @@ def test_slab_range_and_neighbours():
     assert neighbours(0, 4) == (3, 1) and neighbours(3, 4) == (2, 0) and neighbours(0, 2) == (1, 1)
 
 
+def test_split_z_gives_contiguous_plane_blocks():
+    from bgk3d_hit_b200.slabs import split_z
+
+    lx, ly, lz = 3, 2, 12
+    a = np.arange(lx * ly * lz, dtype=float)
+    parts = split_z(a, (lx, ly, lz), 4)
+    assert [p.shape for p in parts] == [(3, 2, 3)] * 4
+    assert np.array_equal(np.concatenate(parts, axis=0).reshape(-1), a)
+    assert parts[1][0, 0, 0] == 3 * lx * ly  # slab 1 starts at global plane 3
+
+
 def test_fp16_scale_for_velocity_bounds_the_stored_values():
     from bgk3d_hit_b200.hit import hit_velocity
     from bgk3d_hit_b200.slabs import fp16_scale_for_velocity, scale_for_max

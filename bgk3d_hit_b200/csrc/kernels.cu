@@ -463,13 +463,18 @@ __global__ void __launch_bounds__(256, 5) k_aa_f16_odd(Pops<__half> a, Geo g, St
 // thread of the cell that owns it in the one-cell-per-thread kernel, or by a
 // lane of the same warp after a shuffle that orders it behind the owner's
 // loads, so the in-place update stays race-free. 128-thread blocks; the even
-// step is capped at 80 registers like k_two_f16v, the odd step, whose shifted
-// accesses need more registers, at 128 (no spills): on B200 at 256^3 that
-// measured 71.0 GLUPS for the pair of steps, against 69.5 with 256-thread
-// blocks, 63.4 with the odd step also capped at 80 registers (282 spilled
-// bytes) and 58 for one cell per thread.
+// step is capped at 80 registers like k_two_f16v. The odd step stores to the
+// rows it loaded from; left alone, the compiler keeps those 18 row addresses
+// live through the collision, so the BGK odd step recomputes them from an
+// opaque copy of (j, k) and fits 96 registers without spills (5 blocks per
+// SM). On B200 at 256^3 the pair of steps measured 72.3 GLUPS, against 71.1
+// with the addresses kept (128 registers, 4 blocks), 69.5 with 256-thread
+// blocks, 63.4 with the odd step capped at 80 registers (282 spilled bytes),
+// 62.8-65.0 with two cells per thread on the odd step, and 58 for one cell per
+// thread. The LES odd step keeps its addresses (4 blocks).
 template <bool ODD, bool LES>
-__global__ void __launch_bounds__(128, ODD ? 4 : 6) k_aa_f16v(Pops<__half> a, Geo g, StepK K, int log_tpr) {
+__global__ void __launch_bounds__(128, ODD ? (LES ? 4 : 5) : 6) k_aa_f16v(Pops<__half> a, Geo g, StepK K,
+                                                                          int log_tpr) {
   const int tpr = 1 << log_tpr;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = t >> log_tpr, pos = t & (tpr - 1);
@@ -498,10 +503,19 @@ __global__ void __launch_bounds__(128, ODD ? 4 : 6) k_aa_f16v(Pops<__half> a, Ge
   }
   if constexpr (LES) collide4_f16_les(Y, K);
   else collide4_f16(Y, K);
+  int js = j, ks = k;  // store rows: recomputed after the collision (BGK odd step)
+  if (ODD && !LES) asm volatile("" : "+r"(js), "+r"(ks));
+  const int jms = js == 0 ? g.ny - 1 : js - 1, jps = js == g.ny - 1 ? 0 : js + 1;
+  const int kms = ks == 0 ? g.nz - 1 : ks - 1, kps = ks == g.nz - 1 ? 0 : ks + 1;
+  auto row_out = [&](int dy, int dz) {
+    const int jj = dy > 0 ? jps : (dy < 0 ? jms : js);
+    const int kk = dz > 0 ? kps : (dz < 0 ? kms : ks);
+    return g.sx * (jj + g.ny * kk);
+  };
 #pragma unroll
   for (int q = 0; q < Q; ++q) {
     if (!ODD) *reinterpret_cast<uint2*>(a.p[oppq(q)] + row(0, 0) + i0) = Y[q];
-    else shift_out(Y[q], cxq(q), a.p[q] + row(cyq(q), czq(q)), i0, i_prev, i_next, xl);
+    else shift_out(Y[q], cxq(q), a.p[q] + row_out(cyq(q), czq(q)), i0, i_prev, i_next, xl);
   }
 }
 
@@ -976,6 +990,12 @@ StepK make_stepk(int form, double omega, double scale, double les_cs) {
 }
 
 // log2(nx/V) when the V-cells-per-thread FP16 kernel applies, else -1.
+// Grid of the FP16 vector kernels: 128-thread blocks over the ny * 2^log_tpr
+// threads of a plane, `planes` planes.
+static dim3 f16v_grid(const Geo& g, int log_tpr, int planes) {
+  return dim3((unsigned)((((long long)g.ny << log_tpr) + 127) / 128), (unsigned)planes);
+}
+
 static int f16v_log_tpr(const Geo& g, int V) {
   if (g.nx % V) return -1;
   const int tpr = g.nx / V;
@@ -998,7 +1018,7 @@ static cudaError_t two_impl(const Lattice& s, const Lattice& d, const StepK& K, 
     if (lt >= 0) {
       Pops<__half> ph = pops_of<__half>(d);
       ph.p[Q - 1] = (__half*)s.p[Q - 1];
-      dim3 grid((unsigned)((((long long)s.g.ny << lt) + 127) / 128), s.g.nz);
+      const dim3 grid = f16v_grid(s.g, lt, s.g.nz);
       k_two_f16v<true><<<grid, 128, 0, st>>>(pops_of<const __half>(s), ph, s.g, K, lt, 0);
     } else {
       k_two<F, true><<<sh.grid, sh.block, 0, st>>>(ps, pd, s.g, K);
@@ -1063,7 +1083,7 @@ static cudaError_t aa_impl(const Lattice& a, int odd, const StepK& K, int varian
   const int lt4 = F::id == FORM_F16 && (variant == 0 || variant == 4) ? f16v_log_tpr(a.g, 4) : -1;
   if (K.les) {
     if (lt4 >= 0) {
-      dim3 grid((unsigned)((((long long)a.g.ny << lt4) + 127) / 128), a.g.nz);
+      const dim3 grid = f16v_grid(a.g, lt4, a.g.nz);
       if (odd) k_aa_f16v<true, true><<<grid, 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
       else k_aa_f16v<false, true><<<grid, 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
     } else if (odd) {
@@ -1080,7 +1100,7 @@ static cudaError_t aa_impl(const Lattice& a, int odd, const StepK& K, int varian
   }
   // FP16: four cells per thread where the box fits it (automatic or 4)
   if (lt4 >= 0) {
-    dim3 grid((unsigned)((((long long)a.g.ny << lt4) + 127) / 128), a.g.nz);
+    const dim3 grid = f16v_grid(a.g, lt4, a.g.nz);
     if (odd) k_aa_f16v<true, false><<<grid, 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
     else k_aa_f16v<false, false><<<grid, 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
     return cudaGetLastError();
@@ -1247,7 +1267,7 @@ static cudaError_t slab_impl(const Lattice& s, const Lattice& d, const StepK& K,
     if (lt >= 0) {
       Pops<__half> ph = pops_of<__half>(d);
       ph.p[Q - 1] = (__half*)s.p[Q - 1];
-      const dim3 gv((unsigned)((((long long)s.g.ny << lt) + 127) / 128), s.g.nz - 2);
+      const dim3 gv = f16v_grid(s.g, lt, s.g.nz - 2);
       if (K.les) k_two_f16v<true><<<gv, 128, 0, st_in>>>(pops_of<const __half>(s), ph, s.g, K, lt, 1);
       else k_two_f16v<false><<<gv, 128, 0, st_in>>>(pops_of<const __half>(s), ph, s.g, K, lt, 1);
     } else {

@@ -11,28 +11,36 @@ boundaries + col_MC). Prints one JSON line.
 
 - value: GLUPS with the populations resident in HBM, K steps timed with CUDA
   events on the library's stream (inputs are 5 GB, larger than L2).
+- forms (default run, one GPU): the same box in FP32-deviation and
+  FP16-scaled-deviation storage (default two-lattice kernels), each timed
+  the same way over max(K, 200) steps with its own clock record, its GLUPS
+  ratio to the FP64 value and its roofline.
+- large (default run, one GPU): FP64 two-lattice at 512^3 (k0 = 6,
+  tau = 0.503) and the AA pattern at 1024^3 in FP16 and FP32 storage (k0 = 8,
+  tau = 0.502), initial field made on the GPU; max(K, 50) steps each, own
+  clock record.
 - e2e: the same K steps through the public C-ABI as a user drives them: the
   initial velocity field uploaded from pinned host memory, then
   boundaries + col_MC + diagnostic every step (diagnostics computed every
   icheck = 100 steps, the reference's default, SRC/input.F90:221, and read
-  back to the host), all inside the timed region.
+  back to the host), all inside the timed region; split into the one-time
+  part (upload + init, fixed_ms) and the per-step part (per_step_ms).
 - roofline: algorithmic bytes of the stream-collide kernel (19 loads + 19
   stores per cell) per launch / average launch time, against the measured HBM
   copy bandwidth.
 - cpu_baseline: the CPU oracle (C restatement of the reference's
   boundaries + col_MC, FP64, OpenMP over all host cores) on a bounded sample.
-- --impl reference: times that CPU implementation on this workload (rank 0).
-Under torchrun, each rank runs an independent replica box on its own GPU
-(the path needs no collective on one box per GPU); value is the sum of the
-ranks' cell updates over the slowest rank's time.
---decomp slabs: one box split along z instead (bgk3d_hit_b200.slabs): under
-torchrun each rank holds one size^3 slab of a size x size x (N size) box
-(weak scaling), the face populations go straight into the neighbours' ghost
-planes over NVLink (CUDA IPC) and a one-element NCCL all-reduce on the
-slab's stream separates the steps; on one GPU, --local-slabs P splits the
-size^3 box into P slabs in one process (the exchange and its host barrier
-measured without a second GPU). The HIT field of each rank's slab is the
-same size^3 tile.
+- --impl reference: times that CPU implementation on this workload (rank 0),
+  with the same config and warm-up as the GPU arm.
+Under torchrun (N > 1) the default is one box split along z (--decomp slabs,
+bgk3d_hit_b200.slabs): each rank holds one size^3 slab of a
+size x size x (N size) box (weak scaling), the face populations go straight
+into the neighbours' ghost planes over NVLink (CUDA IPC) and a one-element
+NCCL all-reduce on the slab's stream separates the steps; value is all
+ranks' cell updates over the slowest rank's time. --decomp replicas runs N
+independent boxes instead. On one GPU, --decomp slabs --local-slabs P
+splits the size^3 box into P slabs in one process (the exchange and its
+barrier measured without a second GPU).
 """
 from __future__ import annotations
 
@@ -70,13 +78,19 @@ def parse():
                     help="stream-collide kernel (0 automatic; 2/4 cells per thread apply to FP16; 8 TMA row pipeline)")
     ap.add_argument("--les-cs", type=float, default=0.0,
                     help="Smagorinsky constant: > 0 times the LES collision instead of BGK")
-    ap.add_argument("--decomp", default="replicas", choices=["replicas", "slabs"],
-                    help="N > 1: independent replica boxes (default) or one box split into z-slabs")
+    ap.add_argument("--decomp", default=None, choices=["replicas", "slabs"],
+                    help="one box split into z-slabs (default under torchrun) or independent replica boxes "
+                         "(default on one GPU)")
     ap.add_argument("--local-slabs", type=int, default=2, help="--decomp slabs on one GPU: slabs per box")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
-    return ap.parse_args()
+    ap.add_argument("--no-forms", action="store_true", help="skip the FP32 / FP16 lines of the default run")
+    ap.add_argument("--no-large", action="store_true", help="skip the 512^3 / 1024^3 lines of the default run")
+    a = ap.parse_args()
+    if a.decomp is None:
+        a.decomp = "slabs" if int(os.environ.get("WORLD_SIZE", "1")) > 1 else "replicas"
+    return a
 
 
 def workload_name(a):
@@ -139,6 +153,47 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows), "power_w_max": max(pw) if pw else None}
 
 
+# ------------------------------------------------------------ shared parts
+N_ARRAYS = {"two_lattice": 37, "aa": 19}
+ELEM = {"fp64": 8, "fp32": 4, "fp16": 2}
+# the larger boxes of the default run: (size, precision, scheme, k0, tau)
+LARGE = ((512, "fp64", "two_lattice", 6.0, 0.503), (1024, "fp16", "aa", 8.0, 0.502),
+         (1024, "fp32", "aa", 8.0, 0.502))
+
+
+def config_of(a, ws):
+    """The run's config dict; both arms print the same one."""
+    L = a.size
+    pop_gb = N_ARRAYS[a.scheme] * ELEM[a.precision] * float(L) ** 3 / 1e9
+    cfg = {"workload": workload_name(a), "box": L, "precision": a.precision, "scheme": a.scheme, "tau": a.tau,
+           "k0": a.k0, "u_rms": 0.03, "seed": 1234, "cells_per_gpu": L ** 3, "kernel": a.kernel,
+           "les_cs": a.les_cs,
+           "l2": f"inputs larger than L2 ({pop_gb:.1f} GB of populations per GPU, L2 126 MB)"
+           if pop_gb > 0.126 else "inputs may fit in L2"}
+    if a.decomp == "slabs":
+        nslab = ws if ws > 1 else a.local_slabs
+        cfg["workload"] += f", split into {nslab} z-slabs"
+        cfg["box"] = [L, L, L * ws if ws > 1 else L]
+        cfg["slabs"] = nslab
+        cfg["parallelism"] = (f"z-slabs, {'one per GPU' if ws > 1 else 'all on one GPU'}, ghost planes filled "
+                              "by the step kernel (peer stores), barrier between steps")
+    else:
+        cfg["parallelism"] = f"{ws} independent replica box(es), one per GPU"
+    return cfg
+
+
+def kernel_key(precision, scheme, L, kernel=0, les=False):
+    """Name of the stream-collide kernel a launch runs (the key of
+    profiles/ncu_traffic.json)."""
+    kern = f"{'k_two' if scheme == 'two_lattice' else 'k_aa'}_{precision}" + ("_les" if les else "")
+    if precision == "fp16" and not les and kernel in ((0, 2, 4) if scheme == "two_lattice" else (0, 4)):
+        v = 2 if kernel == 2 else 4
+        tpr = L // v
+        if L % v == 0 and tpr & (tpr - 1) == 0 and (L * tpr) % 32 == 0:  # cells per thread: 2 or 4
+            kern = ("k_two_f16v2" if kernel == 2 else "k_two_f16v") if scheme == "two_lattice" else "k_aa_f16v"
+    return kern
+
+
 # -------------------------------------------------------------- CPU oracle
 def cpu_baseline(a, seconds: float):
     """The oracle's FP64 boundaries + col_MC (reference algorithm) on the host
@@ -180,7 +235,7 @@ def run_reference(a):
     t1 = orc.time_steps(svisc, 1)
     # each timed step is a bounded sample: cap the whole run at a few minutes
     k = max(1, min(a.steps, int(120.0 / max(t1, 1e-6))))
-    w_ = max(0, min(a.warmup, 2))
+    w_ = max(0, min(a.warmup, int(60.0 / max(t1, 1e-6))))
     orc.time_steps(svisc, w_)
     t = orc.time_steps(svisc, k)
     val = L ** 3 * k / t / 1e9
@@ -189,7 +244,7 @@ def run_reference(a):
         "impl": "reference", "metric": "GLUPS (fused D3Q19 stream-collide)", "value": val, "unit": "GLUPS",
         "n_gpus": ws, "steps": k, "warmup": w_, "ms_per_step": 1e3 * t / k, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": DTYPE["fp64"], "data": "synthetic",
-        "config": {"workload": workload_name(a), "box": L, "precision": "fp64", "scheme": "two_lattice"},
+        "config": config_of(a, ws),
         "cpu_baseline": {"value": val, "unit": "GLUPS", "cores": cores, "kind": "port",
                          "sample": f"{k} steps of {L}^3 FP64, C restatement of boundaries + col_MC "
                                    "(the Fortran/MPI reference cannot be built in this image)"},
@@ -215,6 +270,94 @@ def ncu_traffic(kernel_key: str):
         return None
 
 
+def time_steps(box, steps, device):
+    """K steps of a resident box between CUDA events on its stream, with a
+    clock record of the region: (ms, launches, clocks)."""
+    import torch
+
+    stream = torch.cuda.ExternalStream(box.stream, device=device)
+    clocks = ClockSampler(device)
+    clocks.start()
+    l0 = box.launch_count
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    box.synchronize()
+    e0.record(stream)
+    box.run(steps)
+    e1.record(stream)
+    box.synchronize()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    return ms, box.launch_count - l0, clocks.stop()
+
+
+def roofline_of(precision, scheme, L, ms_per_step, kernel=0, les=False):
+    bpc = BYTES_PER_CELL[precision]
+    peak, peak_kind = measured_hbm()
+    achieved = bpc * float(L) ** 3 / (ms_per_step * 1e-3) / 1e9
+    kern = kernel_key(precision, scheme, L, kernel, les)
+    tr = ncu_traffic(kern)
+    return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": tr * float(L) ** 3 if tr else None, "peak_kind": peak_kind, "bytes_per_cell": bpc,
+            "kernel": kern}
+
+
+def form_line(a, precision, pin, device, fp64_value):
+    """The default box in another storage form (default two-lattice kernel)."""
+    import bgk3d_hit_b200 as B
+
+    L = a.size
+    steps = max(a.steps, 200)
+    box = B.BGK3D(L, svisc=(a.tau - 0.5) / 3.0, u0=0.03, precision=precision, scheme="two_lattice",
+                  icheck=a.icheck, device=device)
+    try:
+        box.init_velocity(*(p.numpy() for p in pin))
+        box.run(a.warmup)
+        ms, launches, clk = time_steps(box, steps, device)
+    finally:
+        box.close()
+    value = float(L) ** 3 * steps / (ms * 1e-3) / 1e9
+    rl = roofline_of(precision, "two_lattice", L, ms / steps)
+    if rl["traffic"] is not None:
+        rl["traffic_note"] = "ncu DRAM bytes per cell of the 256^3 capture x cells"
+    return {"value": value, "unit": "GLUPS", "ratio_vs_fp64": value / fp64_value, "steps": steps,
+            "warmup": a.warmup, "ms_per_step": ms / steps, "dtype": DTYPE[precision], "scheme": "two_lattice",
+            "roofline": rl, "gpu_launches": launches, "clocks": clk}
+
+
+def large_line(a, L, precision, scheme, k0, tau, device):
+    """A larger box of the same path, initial field made on the GPU."""
+    import torch
+
+    import bgk3d_hit_b200 as B
+    from bgk3d_hit_b200.hit import NUMPY_NOISE_MAX_CELLS, hit_velocity_device
+
+    steps = max(a.steps, 50)
+    t0 = time.time()
+    box = B.BGK3D(L, svisc=(tau - 0.5) / 3.0, u0=0.03, precision=precision, scheme=scheme, icheck=a.icheck,
+                  device=device)
+    try:
+        u = hit_velocity_device(L, k0, 0.03, 1234, device=device)
+        box.init_velocity_device(*u)
+        del u
+        torch.cuda.empty_cache()
+        init_s = time.time() - t0
+        box.run(a.warmup)
+        ms, launches, clk = time_steps(box, steps, device)
+        dev_gb = box.device_bytes / 1e9
+    finally:
+        box.close()
+    value = float(L) ** 3 * steps / (ms * 1e-3) / 1e9
+    rl = roofline_of(precision, scheme, L, ms / steps)
+    if rl["traffic"] is not None:
+        rl["traffic_note"] = "ncu DRAM bytes per cell of the 256^3 capture x cells"
+    noise = "numpy default_rng" if L ** 3 <= NUMPY_NOISE_MAX_CELLS else "torch CUDA generator"
+    return {"workload": f"decaying HIT {L}^3 D3Q19 BGK, {precision} {scheme}, tau={tau}, k0={k0:g}, u_rms=0.03, "
+                        f"seed 1234 ({noise} noise)", "box": L, "precision": precision, "scheme": scheme,
+            "value": value, "unit": "GLUPS", "steps": steps, "warmup": a.warmup, "ms_per_step": ms / steps,
+            "device_gb": dev_gb, "init_s": init_s, "roofline": rl, "gpu_launches": launches, "clocks": clk}
+
+
 def run_ours(a):
     import torch
 
@@ -234,6 +377,7 @@ def run_ours(a):
     svisc = (a.tau - 0.5) / 3.0
     u, v, w = hit_velocity(L, a.k0, 0.03, 1234)
     pin = [torch.from_numpy(x).pin_memory() for x in (u, v, w)]
+    del u, v, w
     box = B.BGK3D(L, svisc=svisc, u0=0.03, precision=a.precision, scheme=a.scheme, icheck=a.icheck, device=local,
                   kernel=a.kernel, les_cs=a.les_cs)
     box.init_velocity(*(p.numpy() for p in pin))
@@ -271,23 +415,13 @@ def run_ours(a):
     ms_max = max_over_ranks(ms)
     lu = float(L) ** 3 * a.steps
     value = ws * lu / (ms_max * 1e-3) / 1e9
-    per_launch_s = ms * 1e-3 / a.steps
-    bpc = BYTES_PER_CELL[a.precision]
-    achieved = bpc * float(L) ** 3 / per_launch_s / 1e9
-    peak, peak_kind = measured_hbm()
-    kern = f"{'k_two' if a.scheme == 'two_lattice' else 'k_aa'}_{a.precision}" + ("_les" if a.les_cs > 0 else "")
-    if a.precision == "fp16" and a.les_cs == 0 and a.kernel in ((0, 2, 4) if a.scheme == "two_lattice" else (0, 4)):
-        v = 2 if a.kernel == 2 else 4
-        tpr = L // v
-        if L % v == 0 and tpr & (tpr - 1) == 0 and (L * tpr) % 32 == 0:  # cells per thread: 2 or 4
-            kern = ("k_two_f16v2" if a.kernel == 2 else "k_two_f16v") if a.scheme == "two_lattice" else "k_aa_f16v"
-    tr = ncu_traffic(kern)
-    traffic = tr * float(L) ** 3 if tr else None
+    roofline = roofline_of(a.precision, a.scheme, L, ms / a.steps, a.kernel, a.les_cs > 0)
+    box.close()
 
     # -------- e2e through the C-ABI with host buffers
     e2e = None
     if not a.no_e2e:
-        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0, evi, ev1 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
         box2 = B.BGK3D(L, svisc=svisc, u0=0.03, precision=a.precision, scheme=a.scheme, icheck=a.icheck,
                        device=local, kernel=a.kernel, les_cs=a.les_cs)
         stream2 = torch.cuda.ExternalStream(box2.stream, device=local)
@@ -296,6 +430,7 @@ def run_ours(a):
             torch.distributed.barrier()
         ev0.record(stream2)
         box2.init_velocity(*(p.numpy() for p in pin))
+        evi.record(stream2)
         ndiag = 0
         for it in range(1, a.steps + 1):
             box2.boundaries(it)
@@ -307,13 +442,36 @@ def run_ours(a):
         ev1.record(stream2)
         box2.synchronize()
         ms2 = max_over_ranks(ev0.elapsed_time(ev1))
+        fixed = max_over_ranks(ev0.elapsed_time(evi))
+        per_step = (ms2 - fixed) / a.steps
         diag_bytes = 11 * 8
         e2e = {"value": ws * lu / (ms2 * 1e-3) / 1e9, "unit": "GLUPS",
                "h2d_bytes_per_step": 3 * 8 * L ** 3 / a.steps,
                "d2h_bytes_per_step": diag_bytes * ndiag / a.steps,
-               "includes": f"velocity upload from pinned host memory, {a.steps} x (boundaries + col_MC + "
-                           f"diagnostic gated by icheck={a.icheck}), diagnostics read back"}
+               "fixed_ms": fixed, "per_step_ms": per_step,
+               "value_at_2000_steps": ws * float(L) ** 3 * 2000 / ((fixed + 2000 * per_step) * 1e-3) / 1e9,
+               "includes": f"velocity upload from pinned host memory and init (fixed_ms), {a.steps} x "
+                           f"(boundaries + col_MC + diagnostic gated by icheck={a.icheck}), diagnostics read back "
+                           "(per_step_ms); value_at_2000_steps = the same split at the 2000 steps of the HIT "
+                           "256^3 run"}
         box2.close()
+
+    default_run = (ws == 1 and a.precision == "fp64" and a.scheme == "two_lattice" and a.les_cs == 0
+                   and a.kernel == 0)
+    forms = None
+    if default_run and not a.no_forms:
+        forms = {"fp64": {"value": value, "unit": "GLUPS", "ratio_vs_fp64": 1.0, "note": "the headline line"}}
+        for prec in ("fp32", "fp16"):
+            forms[prec] = form_line(a, prec, pin, local, value)
+    large = None
+    if default_run and not a.no_large:
+        large = []
+        for (Lb, prec, sch, k0, tau) in LARGE:
+            try:
+                large.append(large_line(a, Lb, prec, sch, k0, tau, local))
+            except Exception as ex:  # a box that does not fit is reported, not fatal
+                large.append({"box": Lb, "precision": prec, "scheme": sch, "error": str(ex)[:200]})
+            torch.cuda.empty_cache()
 
     cpu = None
     if rank == 0 and ws == 1 and not a.no_cpu:
@@ -327,17 +485,14 @@ def run_ours(a):
             "metric": "GLUPS (fused D3Q19 stream-collide)", "value": value, "unit": "GLUPS", "n_gpus": ws,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_max / a.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": DTYPE[a.precision], "data": "synthetic",
-            "config": {"workload": workload_name(a), "box": L, "precision": a.precision, "scheme": a.scheme,
-                       "tau": a.tau, "cells_per_gpu": L ** 3, "kernel": a.kernel,
-                       "l2": f"inputs larger than L2 ({box.device_bytes / 1e9:.1f} GB resident, L2 126 MB)",
-                       "parallelism": f"{ws} independent replica box(es), one per GPU"},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic,
-                         "peak_kind": peak_kind, "bytes_per_cell": bpc, "kernel": kern},
-            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk,
+            "config": config_of(a, ws), "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": launches, "clocks": clk,
         }
+        if forms is not None:
+            line["forms"] = forms
+        if large is not None:
+            line["large"] = large
         print(json.dumps(line), flush=True)
-    box.close()
     if ws > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
@@ -401,20 +556,21 @@ def run_slabs(a):
     bpc = BYTES_PER_CELL[a.precision]
     peak, peak_kind = measured_hbm()
     achieved = bpc * (cells / ws) / (ms * 1e-3 / a.steps) / 1e9
+    # per step, every slab stores 5 populations of each of its two boundary
+    # planes into its neighbours' ghost planes
+    exch = len(boxes) * 2 * 5 * L * L * ELEM[a.precision]
     if rank == 0:
         line = {
             "metric": "GLUPS (fused D3Q19 stream-collide)", "value": value, "unit": "GLUPS", "n_gpus": ws,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms / a.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": DTYPE[a.precision], "data": "synthetic",
-            "config": {"workload": workload_name(a) + f", split into {nslab} z-slabs",
-                       "box": [L, L, L * ws if ws > 1 else L], "precision": a.precision, "scheme": a.scheme,
-                       "tau": a.tau, "slabs": nslab, "gpus": ws,
-                       "l2": "inputs larger than L2" if cells * bpc / ws > 126e6 else "inputs may fit in L2",
-                       "parallelism": f"z-slabs, {'one per GPU' if ws > 1 else 'all on one GPU'}, ghost planes "
-                                      "filled by the step kernel (peer stores), barrier between steps"},
+            "config": config_of(a, ws),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind, "bytes_per_cell": bpc,
                          "kernel": f"k_slab_{a.precision}", "per": "whole step of this GPU's slabs"},
+            "exchange": {"bytes_per_step_per_gpu": exch, "peer": ws > 1,
+                         "what": "2 faces x 5 populations x lx*ly x element size per slab, stored by the edge "
+                                 "kernel into the neighbours' ghost planes"},
             "cpu_baseline": None, "e2e": None, "gpu_launches": launches, "clocks": clk,
         }
         print(json.dumps(line), flush=True)

@@ -225,6 +225,78 @@ int sync_and_check(bgk_ctx* c) {
   return BGK_OK;
 }
 
+// Equilibrium initial condition from a velocity field: host arrays go
+// through a staging buffer in chunks of whole planes; device arrays (on the
+// context's device) are read in place, chunk by chunk in the same order.
+int init_velocity_impl(bgk_ctx* c, const double* u, const double* v, const double* w, double rho, bool on_device) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!u || !v || !w) {
+    set_err("null velocity array");
+    return BGK_ERR_INVALID;
+  }
+  if (!(rho > 0.0) || !std::isfinite(rho)) {
+    set_err("rho must be positive and finite, got %g", rho);
+    return BGK_ERR_INVALID;
+  }
+  CK(cudaSetDevice(c->p.device));
+  if (on_device) {
+    for (const double* p : {u, v, w}) {
+      cudaPointerAttributes at{};
+      CK(cudaPointerGetAttributes(&at, p));
+      if ((at.type != cudaMemoryTypeDevice && at.type != cudaMemoryTypeManaged) || at.device != c->p.device) {
+        set_err("velocity arrays must be device memory of device %d", c->p.device);
+        return BGK_ERR_INVALID;
+      }
+    }
+  }
+  const long long plane = (long long)c->g.nx * c->g.ny;
+  int nk = (int)(INIT_CHUNK_CELLS / plane);
+  if (nk < 1) nk = 1;
+  if (nk > c->g.nz) nk = c->g.nz;
+  const size_t chunk = (size_t)plane * nk;
+  double *su = nullptr, *sv = nullptr, *sw = nullptr;
+  if (!on_device) {
+    rc = ensure_stage(c, 3 * chunk * sizeof(double));
+    if (rc) return rc;
+    su = (double*)c->stage;
+    sv = su + chunk;
+    sw = sv + chunk;
+  }
+  const int lay = init_layout(c);
+  const bool measure = c->form == FORM_F16 && c->p.fp16_scale == 0.0;
+  if (measure) CK(cudaMemsetAsync(c->d_max, 0, sizeof(unsigned int), c->st));
+  for (int pass = measure ? 0 : 1; pass < 2; ++pass) {
+    if (pass == 1 && measure) {
+      rc = set_scale_from_max(c);
+      if (rc) return rc;
+    }
+    for (int k0 = 0; k0 < c->g.nz; k0 += nk) {
+      const int nkk = k0 + nk <= c->g.nz ? nk : c->g.nz - k0;
+      const size_t off = (size_t)plane * k0, cnt = (size_t)plane * nkk * sizeof(double);
+      if (on_device) {
+        su = const_cast<double*>(u) + off;
+        sv = const_cast<double*>(v) + off;
+        sw = const_cast<double*>(w) + off;
+      } else {
+        CK(cudaMemcpyAsync(su, u + off, cnt, cudaMemcpyHostToDevice, c->st));
+        CK(cudaMemcpyAsync(sv, v + off, cnt, cudaMemcpyHostToDevice, c->st));
+        CK(cudaMemcpyAsync(sw, w + off, cnt, cudaMemcpyHostToDevice, c->st));
+      }
+      CK(launch_init_velocity(c->A, lay, su, sv, sw, rho, k0, nkk, pass == 0 ? 1.0 : c->scale,
+                              pass == 0 ? c->d_max : nullptr, c->st));
+      c->launches++;
+    }
+  }
+  CK(cudaMemsetAsync(c->d_err, 0, sizeof(int), c->st));
+  CK(cudaStreamSynchronize(c->st));
+  c->lay = lay;
+  c->step = 0;
+  c->initialized = 1;
+  c->primed = 0;
+  return BGK_OK;
+}
+
 int compute_diag(bgk_ctx* c, int itime, bgk_diag* out, int want_extras) {
   const bool extras = want_extras && c->p.extras && !c->slab;
   if (extras) {
@@ -525,53 +597,11 @@ int bgk_init_tgv(bgk_ctx* c) {
 }
 
 int bgk_init_velocity(bgk_ctx* c, const double* u, const double* v, const double* w, double rho) {
-  int rc = check_ctx(c);
-  if (rc) return rc;
-  if (!u || !v || !w) {
-    set_err("null velocity array");
-    return BGK_ERR_INVALID;
-  }
-  if (!(rho > 0.0) || !std::isfinite(rho)) {
-    set_err("rho must be positive and finite, got %g", rho);
-    return BGK_ERR_INVALID;
-  }
-  CK(cudaSetDevice(c->p.device));
-  const long long plane = (long long)c->g.nx * c->g.ny;
-  int nk = (int)(INIT_CHUNK_CELLS / plane);
-  if (nk < 1) nk = 1;
-  if (nk > c->g.nz) nk = c->g.nz;
-  const size_t chunk = (size_t)plane * nk;
-  rc = ensure_stage(c, 3 * chunk * sizeof(double));
-  if (rc) return rc;
-  double* su = (double*)c->stage;
-  double* sv = su + chunk;
-  double* sw = sv + chunk;
-  const int lay = init_layout(c);
-  const bool measure = c->form == FORM_F16 && c->p.fp16_scale == 0.0;
-  if (measure) CK(cudaMemsetAsync(c->d_max, 0, sizeof(unsigned int), c->st));
-  for (int pass = measure ? 0 : 1; pass < 2; ++pass) {
-    if (pass == 1 && measure) {
-      rc = set_scale_from_max(c);
-      if (rc) return rc;
-    }
-    for (int k0 = 0; k0 < c->g.nz; k0 += nk) {
-      const int nkk = k0 + nk <= c->g.nz ? nk : c->g.nz - k0;
-      const size_t off = (size_t)plane * k0, cnt = (size_t)plane * nkk * sizeof(double);
-      CK(cudaMemcpyAsync(su, u + off, cnt, cudaMemcpyHostToDevice, c->st));
-      CK(cudaMemcpyAsync(sv, v + off, cnt, cudaMemcpyHostToDevice, c->st));
-      CK(cudaMemcpyAsync(sw, w + off, cnt, cudaMemcpyHostToDevice, c->st));
-      CK(launch_init_velocity(c->A, lay, su, sv, sw, rho, k0, nkk, pass == 0 ? 1.0 : c->scale,
-                              pass == 0 ? c->d_max : nullptr, c->st));
-      c->launches++;
-    }
-  }
-  CK(cudaMemsetAsync(c->d_err, 0, sizeof(int), c->st));
-  CK(cudaStreamSynchronize(c->st));
-  c->lay = lay;
-  c->step = 0;
-  c->initialized = 1;
-  c->primed = 0;
-  return BGK_OK;
+  return init_velocity_impl(c, u, v, w, rho, false);
+}
+
+int bgk_init_velocity_device(bgk_ctx* c, const double* u, const double* v, const double* w, double rho) {
+  return init_velocity_impl(c, u, v, w, rho, true);
 }
 
 int bgk_boundaries(bgk_ctx* c, int itime) {

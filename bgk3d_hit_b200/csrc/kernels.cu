@@ -989,13 +989,13 @@ StepK make_stepk(int form, double omega, double scale, double les_cs) {
   return k;
 }
 
-// log2(nx/V) when the V-cells-per-thread FP16 kernel applies, else -1.
 // Grid of the FP16 vector kernels: 128-thread blocks over the ny * 2^log_tpr
 // threads of a plane, `planes` planes.
 static dim3 f16v_grid(const Geo& g, int log_tpr, int planes) {
   return dim3((unsigned)((((long long)g.ny << log_tpr) + 127) / 128), (unsigned)planes);
 }
 
+// log2(nx/V) when the V-cells-per-thread FP16 kernel applies, else -1.
 static int f16v_log_tpr(const Geo& g, int V) {
   if (g.nx % V) return -1;
   const int tpr = g.nx / V;

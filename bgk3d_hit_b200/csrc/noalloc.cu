@@ -19,7 +19,6 @@
 
 #include <cmath>
 #include <cstdio>
-#include <mutex>
 
 #include "bgk3d.h"
 #include "kernels.h"
@@ -38,10 +37,6 @@ static_assert(NOALLOC_SCRATCH_BYTES == 94808, "scratch size stated in the header
 // device address: kernels get the address from cudaGetSymbolAddress.
 static __device__ __align__(256) double g_noalloc_scratch[NOALLOC_SCRATCH_DOUBLES];
 
-constexpr int NOALLOC_MAX_DEVICES = 64;
-std::mutex g_noalloc_mu;
-double* g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {};
-
 // Records the message for bgk_last_error() and returns the code.
 int fail(int code, const char* msg) {
   char buf[256];
@@ -50,21 +45,20 @@ int fail(int code, const char* msg) {
   return code;
 }
 
-// Device address of the scratch on the current device, looked up once per
-// device (with that device current) and cached.
-int scratch_on_current_device(double** out) {
-  int dev = -1;
-  cudaError_t e = cudaGetDevice(&dev);
+// Device address of the scratch in the current context, looked up on every
+// call. The lookup is a host-side table query once the module is loaded in
+// the context, so nothing is cached: a cached address would go stale after a
+// cudaDeviceReset (the module is loaded again, possibly elsewhere) and would
+// belong to the wrong context for a caller whose current context is not the
+// device's primary one (one made through the driver API by another runtime).
+// The first call in a context loads the module there, which is why that first
+// call must come before any stream capture.
+int scratch_in_current_context(double** out) {
+  void* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
   if (e != cudaSuccess) return fail(BGK_ERR_CUDA, cudaGetErrorString(e));
-  if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return fail(BGK_ERR_INVALID, "device ordinal beyond 63");
-  std::lock_guard<std::mutex> lock(g_noalloc_mu);
-  if (!g_noalloc_ptr[dev]) {
-    void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess || !p) return fail(BGK_ERR_CUDA, e != cudaSuccess ? cudaGetErrorString(e) : "null scratch");
-    g_noalloc_ptr[dev] = (double*)p;
-  }
-  *out = g_noalloc_ptr[dev];
+  if (!p) return fail(BGK_ERR_CUDA, "null scratch address");
+  *out = (double*)p;
   return BGK_OK;
 }
 
@@ -89,7 +83,7 @@ extern "C" int bgk_diagnostics_noalloc(const void* const* pops19, int lx, int ly
     scale = fp16_scale;
   }
   double* scratch = nullptr;
-  int rc = scratch_on_current_device(&scratch);
+  int rc = scratch_in_current_context(&scratch);
   if (rc) return rc;
   double* partials = scratch;
   double* totals = scratch + NOALLOC_PARTIALS;
@@ -139,5 +133,11 @@ extern "C" int bgk_diagnostics_noalloc(const void* const* pops19, int lx, int ly
   out->eps_strain = t[7] / N;
   out->enstrophy = 0.0;  // needs a 3-component velocity field: not computed here
   out->nonfinite = (long long)t[8];
-  return out->nonfinite > 0 ? BGK_ERR_NONFINITE : BGK_OK;
+  if (out->nonfinite > 0) {
+    char msg[160];
+    std::snprintf(msg, sizeof(msg), "%lld cells with non-finite density or velocity at itime %d", out->nonfinite,
+                  itime);
+    return fail(BGK_ERR_NONFINITE, msg);
+  }
+  return BGK_OK;
 }

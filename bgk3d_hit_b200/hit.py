@@ -14,8 +14,14 @@ per-component rms velocity sqrt(<|u|^2>/3) equals u_rms:
 4. inverse FFT and rescaling to u_rms.
 
 Arrays are (nz, ny, nx) in C order, i.e. Fortran order with i fastest, the
-layout the C-ABI expects. The generator is set-up code (host, FP64); the
-velocity field is handed to ``bgk_init_velocity``.
+layout the C-ABI expects. ``hit_velocity`` is set-up code (host, FP64); its
+field is handed to ``bgk_init_velocity``. ``hit_velocity_device`` runs steps
+2-4 on the GPU (torch.fft, FP64) and leaves the field there for
+``bgk_init_velocity_device``: fed numpy's noise it gives the host field to
+rounding (the FFT libraries differ); above 512^3 cells it draws the noise on
+the GPU too (torch's generator seeded with the same seed: a field with the
+same statistics, not the same realisation), since numpy's noise alone would
+take minutes and three host arrays of 8 GB at 1024^3.
 """
 from __future__ import annotations
 
@@ -75,3 +81,71 @@ def divergence_spectral(u, v, w) -> float:
     kx = np.fft.rfftfreq(nx, 1.0 / nx).reshape(1, 1, nx // 2 + 1)
     d = 1j * (kx * _rfftn(u) + ky * _rfftn(v) + kz * _rfftn(w))
     return float(np.max(np.abs(_irfftn(d, (nz, ny, nx)))))
+
+
+NUMPY_NOISE_MAX_CELLS = 512 ** 3
+
+
+def hit_velocity_device(n: int | tuple, k0: float, u_rms: float, seed: int, device=0, noise: str = "auto"):
+    """The generator of ``hit_velocity`` on the GPU. Returns (u, v, w), float64
+    torch tensors of shape (nz, ny, nx) on ``device``. noise: "numpy" (the
+    host generator's white noise, uploaded), "device" (torch's CUDA generator
+    seeded with ``seed``) or "auto" (numpy up to 512^3 cells)."""
+    import torch
+
+    nz, ny, nx = (n, n, n) if np.isscalar(n) else tuple(n)
+    dev = torch.device("cuda", device) if isinstance(device, int) else torch.device(device)
+    if noise == "auto":
+        noise = "numpy" if nx * ny * nz <= NUMPY_NOISE_MAX_CELLS else "device"
+    if noise == "numpy":
+        rng = np.random.default_rng(seed)
+
+        def white():
+            return torch.from_numpy(rng.standard_normal((nz, ny, nx))).to(dev)
+    elif noise == "device":
+        gen = torch.Generator(device=dev)
+        gen.manual_seed(seed)
+
+        def white():
+            return torch.randn((nz, ny, nx), generator=gen, dtype=torch.float64, device=dev)
+    else:
+        raise ValueError(noise)
+    f64 = dict(dtype=torch.float64, device=dev)
+    kz = torch.fft.fftfreq(nz, 1.0 / nz, **f64).reshape(nz, 1, 1)
+    ky = torch.fft.fftfreq(ny, 1.0 / ny, **f64).reshape(1, ny, 1)
+    kx = torch.fft.rfftfreq(nx, 1.0 / nx, **f64).reshape(1, 1, nx // 2 + 1)
+    k2 = kx * kx + ky * ky + kz * kz
+    amp = torch.sqrt(k2)
+    amp = amp * torch.exp(-((amp / k0) ** 2))
+    for kk, nn in ((kx, nx), (ky, ny), (kz, nz)):
+        if nn % 2 == 0:
+            amp = torch.where(torch.abs(kk) == nn // 2, torch.zeros((), **f64), amp)
+    hat = []
+    for _ in range(3):
+        f = torch.fft.rfftn(white(), dim=(0, 1, 2))
+        mod = torch.abs(f)
+        mod = torch.where(mod == 0, torch.ones((), **f64), mod)
+        f /= mod
+        f *= amp
+        del mod
+        hat.append(f)
+    del amp
+    k2 = torch.where(k2 == 0, torch.ones((), **f64), k2)
+    div = kx * hat[0]
+    div += ky * hat[1]
+    div += kz * hat[2]
+    div /= k2
+    del k2
+    out = []
+    for h, kk in zip(hat, (kx, ky, kz)):
+        h -= kk * div
+        h[0, 0, 0] = 0.0
+    del div
+    for i in range(3):
+        out.append(torch.fft.irfftn(hat[i], s=(nz, ny, nx), dim=(0, 1, 2)))
+        hat[i] = None
+    ms = sum(float(torch.mean(x * x)) for x in out)
+    s = u_rms / float(np.sqrt(ms / 3.0))
+    for x in out:
+        x *= s
+    return tuple(out)

@@ -119,6 +119,17 @@ class BGK3D:
         check(self._lib.bgk_init_velocity(self._h, a[0].ctypes.data_as(dp), a[1].ctypes.data_as(dp),
                                           a[2].ctypes.data_as(dp), rho), "bgk_init_velocity")
 
+    def init_velocity_device(self, u, v, w, rho: float = 1.0):
+        """Equilibrium from a velocity field already on the box's GPU: three
+        contiguous float64 torch tensors of shape (lz, ly, lx), read in place
+        (bgk_init_velocity_device)."""
+        lx, ly, lz = self.shape
+        for t in (u, v, w):
+            if tuple(t.shape) != (lz, ly, lx) or str(t.dtype) != "torch.float64" or not t.is_contiguous():
+                raise ValueError(f"expected contiguous float64 tensors of shape {(lz, ly, lx)}")
+        check(self._lib.bgk_init_velocity_device(self._h, C.c_void_p(u.data_ptr()), C.c_void_p(v.data_ptr()),
+                                                 C.c_void_p(w.data_ptr()), rho), "bgk_init_velocity_device")
+
     # -------------------------------------------------------- time loop
     def boundaries(self, itime: int):
         check(self._lib.bgk_boundaries(self._h, itime), "bgk_boundaries")

@@ -144,6 +144,14 @@ int bgk_init_tgv(bgk_ctx* ctx);
    arithmetic of SRC/init.F90:97-137 with crho = rho. Used for decaying HIT. */
 int bgk_init_velocity(bgk_ctx* ctx, const double* u, const double* v, const double* w, double rho);
 
+/* Same as bgk_init_velocity with the three velocity arrays in device memory
+   of the context's device (lx*ly*lz doubles each, Fortran order), read in
+   place: no host copy and no staging buffer. For fields made on the GPU
+   (large HIT boxes) or held by a device runtime. Arrays of another device or
+   host memory are rejected with BGK_ERR_INVALID. No reference counterpart
+   (SRC/init.F90 builds its field on the host). */
+int bgk_init_velocity_device(bgk_ctx* ctx, const double* u, const double* v, const double* w, double rho);
+
 /* = boundaries(itime) (SRC/boundaries.F90:23-107, default STEP3 variant
    SRC/bcond.comm.step3.F90:29-316). The single periodic box needs no halo
    exchange: every kernel wraps its indices. Kept so that the call sequence is
@@ -323,7 +331,10 @@ int bgk_shift3(const void* in1, const void* in2, const void* in3, void* out1, vo
    Computes the bgk_diagnostic fields except enstrophy (left 0) over caller-
    owned device populations in the reference's meaning: pops19[q] is the
    device base of population q, cell (i,j,k) at i + pitch_x*(j + ly*k), stored
-   as `precision` (FP16: scale fp16_scale). svisc and omega enter the
+   as `precision` (FP16: scale fp16_scale). Only the rows may be padded
+   (pitch_x >= lx); planes follow each other every pitch_x*ly cells, so a
+   driver that keeps the reference's ghosted (0:l+1, 0:m+1, 0:n+1) arrays
+   passes a copy of their interior, not the ghosted arrays themselves. svisc and omega enter the
    dissipation and strain sums, u0 and itime the dissipation.dat columns, mode
    the diagno ztot convention. Runs on the calling thread's current device and
    on `stream` (NULL: default stream), then synchronises that stream.
@@ -332,9 +343,11 @@ int bgk_shift3(const void* in1, const void* in2, const void* in3, void* out1, vo
    pitch_x*ly*lz < 2^31 cells per population and larger ones are rejected with
    BGK_ERR_INVALID. The array keeps the last call's contents; every slot is
    rewritten before it is read, but calls that overlap on the GPU (concurrent
-   streams, threads) race on it. The first call on a device looks up the
-   array's device address (cudaGetSymbolAddress): make that first call before
-   any stream capture. Calls no cudaMalloc or cudaFree. */
+   streams, threads) race on it. Every call looks up the array's device
+   address in the calling thread's current context (cudaGetSymbolAddress);
+   the first call in a context also loads the library's kernels there, so
+   make that first call before any stream capture. Calls no cudaMalloc or
+   cudaFree. */
 int bgk_diagnostics_noalloc(const void* const* pops19, int lx, int ly, int lz, int pitch_x, int precision,
                             double svisc, double omega, double u0, double fp16_scale, int mode, int itime,
                             bgk_diag* out, void* stream);

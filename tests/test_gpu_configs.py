@@ -1,0 +1,172 @@
+"""Parity and accuracy at the benchmarked configurations, through the C-ABI.
+
+- Decaying HIT 256^3 (k0 = 4, u_rms = 0.03, tau = 0.505, seed 1234; the box
+  the FP64 GLUPS figure is measured on), FP64, two-lattice and AA, 10 steps:
+  bit-exact against the oracle stepped in its ghost-fill form, i.e. the
+  reference's loop body boundaries (bcond_comm_step3's z, x, y face copies,
+  SRC/bcond.comm.step3.F90:77-297) + col_MC on the ghosted lattice
+  (SRC/bgk3d_HIT.F90:131,140), not the oracle's modulo shortcut. Diagnostics
+  after 10 steps within 1e-12 relative of the oracle's.
+- Rows of 1024 cells (the 1024^3 AA box's row length: 256 threads, eight
+  warps per row in the four-cells-per-thread FP16 kernels), FP16 and FP32,
+  AA and two-lattice: bit-exact against the oracle over steps of both AA
+  parities.
+- The accuracy bar of the reduced-precision forms: HIT 128^3 (k0 = 4,
+  u_rms = 0.03, tau = 0.51), 600 steps, FP32 and FP16 storage against the FP64
+  run, both schemes: maximum relative error of E(t) (mean 0.5|u|^2) and of
+  eps(t) (2 nu <S:S>) over the run <= 1e-3, and of the final shell spectrum
+  E(k) on shells holding >= 1e-6 of the peak <= 2e-3 (FP32) / 2e-2 (FP16).
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+FORMS = {"fp64": "f64", "fp32": "f32", "fp16": "f16"}
+
+
+def same_bits(a, b):
+    return np.array_equal(np.ascontiguousarray(a).view(np.uint8), np.ascontiguousarray(b).view(np.uint8))
+
+
+def test_hit256_fp64_bitexact_vs_ghost_fill_oracle(bgk, oracle_mod):
+    from bgk3d_hit_b200.hit import hit_velocity
+
+    n, svisc, u0 = 256, 0.005 / 3, 0.03
+    u = hit_velocity(n, 4, u0, 1234)
+    orc = oracle_mod.OracleLattice(n, n, n, form="f64")
+    orc.init_velocity(*u)
+    boxes = {s: bgk.BGK3D(n, svisc=svisc, u0=u0, precision="fp64", scheme=s, icheck=10)
+             for s in ("two_lattice", "aa")}
+    try:
+        for b in boxes.values():
+            b.init_velocity(*u)
+        del u
+        for it in range(1, 11):
+            orc.step(svisc)  # boundaries (step3 ghost fill) + col_MC on ghosts
+            for b in boxes.values():
+                b.boundaries(it)
+                b.col_MC(it)
+            if it in (1, 10):
+                ref = orc.get_pops()
+                for s, b in boxes.items():
+                    assert same_bits(b.populations(), ref), f"{s} after {it} steps"
+                del ref
+        dg = orc.diagno(False)
+        ds = orc.dissipation(svisc, u0, 10, False)
+        for s, b in boxes.items():
+            d = b.diagnostic(10)
+            got = [d["rho_mean"], d["ux_mean"], d["uy_mean"], d["uz_mean"], d["ke_mean"]]
+            np.testing.assert_allclose(got, dg, rtol=1e-12, atol=1e-15, err_msg=s)
+            np.testing.assert_allclose([d["tke_norm"], d["diss"], d["tke"]], ds[1:], rtol=1e-12, atol=1e-15,
+                                       err_msg=s)
+    finally:
+        orc.close()
+        for b in boxes.values():
+            b.close()
+
+
+@pytest.mark.parametrize("form", ["fp16", "fp32"])
+@pytest.mark.parametrize("scheme", ["aa", "two_lattice"])
+@pytest.mark.parametrize("shape", [(1024, 4, 4), (1024, 8, 6)])
+def test_row_length_1024_bitexact(bgk, oracle_mod, form, scheme, shape):
+    from bgk3d_hit_b200.hit import hit_velocity
+
+    nx, ny, nz = shape
+    svisc = 0.002 / 3  # tau = 0.502
+    u = hit_velocity((nz, ny, nx), 8, 0.03, 1234)
+    box = bgk.BGK3D(nx, ny, nz, svisc=svisc, u0=0.03, precision=form, scheme=scheme)
+    box.init_velocity(*u)
+    orc = oracle_mod.OracleLattice(nx, ny, nz, form=FORMS[form], scale=box.scale)
+    orc.init_velocity(*u)
+    try:
+        assert same_bits(box.populations(), orc.get_pops()), "initial state"
+        for it in range(1, 7):
+            orc.step(svisc, periodic=True)
+            box.col_MC(it)
+            if it in (1, 2, 5, 6):
+                assert same_bits(box.populations(), orc.get_pops()), f"after {it} steps"
+    finally:
+        orc.close()
+        box.close()
+
+
+@pytest.mark.parametrize("scheme", ["two_lattice", "aa"])
+def test_reduced_precision_accuracy_bar(bgk, scheme):
+    from bgk3d_hit_b200 import precision_study
+
+    res = precision_study.run(size=128, steps=600, every=25, k0=4.0, tau=0.51, scheme=scheme)
+    assert res["compared_up_to_step"] == 600
+    for f, ek_bound in (("fp32", 2e-3), ("fp16", 2e-2)):
+        r = res["forms"][f]
+        assert r["blowup_step"] is None, f
+        assert r["E_max_rel_err"] <= 1e-3, (f, r)
+        assert r["eps_max_rel_err"] <= 1e-3, (f, r)
+        assert r["Ek_max_rel_err"] <= ek_bound, (f, r)
+        assert r["Ek_shells"] >= 20, (f, r)
+    assert res["forms"]["fp64"]["E_last"] < res["forms"]["fp64"]["E_initial"]
+
+
+@pytest.mark.parametrize("shape", [(64, 64, 64), (24, 20, 16)])
+def test_device_hit_generator_matches_host(shape):
+    """Fed numpy's noise, the GPU generator (torch.fft) gives the host
+    generator's field to 1e-12 of its largest value (the FFT libraries round
+    differently)."""
+    from bgk3d_hit_b200.hit import hit_velocity, hit_velocity_device
+
+    nz, ny, nx = shape
+    host = hit_velocity((nz, ny, nx), 4, 0.03, 1234)
+    dev = hit_velocity_device((nz, ny, nx), 4, 0.03, 1234, device=0, noise="numpy")
+    for h, d in zip(host, dev):
+        assert np.abs(d.cpu().numpy() - h).max() <= 1e-12 * np.abs(h).max()
+
+
+def test_device_noise_field_statistics():
+    """With the noise drawn on the GPU (the generator's choice above 512^3
+    cells), the field still has the requested rms, is solenoidal and peaks in
+    the requested shell."""
+    import torch
+
+    from bgk3d_hit_b200.hit import divergence_spectral, hit_velocity_device
+
+    n, k0 = 96, 6
+    u = hit_velocity_device(n, k0, 0.03, 1234, device=0, noise="device")
+    urms = float(torch.sqrt(sum(torch.mean(x * x) for x in u) / 3))
+    assert urms == pytest.approx(0.03, rel=1e-12)
+    h = [x.cpu().numpy() for x in u]
+    assert divergence_spectral(*h) < 1e-13
+    uh = [np.fft.fftn(x) for x in h]
+    e = sum(np.abs(x) ** 2 for x in uh)
+    k = np.fft.fftfreq(n, 1.0 / n)
+    kk = np.rint(np.sqrt(k[:, None, None] ** 2 + k[None, :, None] ** 2 + k[None, None, :] ** 2)).astype(int)
+    ek = np.bincount(kk.ravel(), e.ravel())
+    assert abs(int(np.argmax(ek)) - k0) <= 1
+    again = hit_velocity_device(n, k0, 0.03, 1234, device=0, noise="device")
+    assert all(torch.equal(x, y) for x, y in zip(u, again))
+
+
+@pytest.mark.parametrize("form", ["fp64", "fp32", "fp16"])
+@pytest.mark.parametrize("scheme", ["two_lattice", "aa"])
+def test_init_velocity_device_equals_host_init(bgk, form, scheme):
+    """bgk_init_velocity_device reads the field in place and gives the same
+    populations, bit for bit, as bgk_init_velocity from host arrays (the
+    FP16 scale chosen the same way), on a box larger than one staging chunk."""
+    import torch
+
+    from bgk3d_hit_b200.hit import hit_velocity
+
+    shape = (160, 128, 1040)  # (lx, ly, lz): 21.3M cells, two chunks of whole planes
+    lx, ly, lz = shape
+    u = hit_velocity((lz, ly, lx), 6, 0.03, 7)
+    a = bgk.BGK3D(*shape, precision=form, scheme=scheme)
+    b = bgk.BGK3D(*shape, precision=form, scheme=scheme)
+    try:
+        a.init_velocity(*u)
+        b.init_velocity_device(*(torch.from_numpy(x).cuda() for x in u))
+        assert a.scale == b.scale
+        assert same_bits(a.populations(), b.populations())
+        with pytest.raises(bgk._abi.BgkError):
+            b.init_velocity_device(*(torch.from_numpy(x) for x in u))  # host memory is rejected
+    finally:
+        a.close()
+        b.close()

@@ -1,16 +1,22 @@
 """bgk_diagnostics_noalloc: diagnostics for callers that cannot allocate.
 
 Some callers cannot let the library call cudaMalloc once their time loop runs
-(their device memory all belongs to another runtime or to their own pool, and
-cudaMalloc can fail on a full device and synchronises it). This entry point
-reduces caller-owned device populations with only a fixed file-scope device
-scratch array. Here it must give the same diagnostics as the context entry
-point (bgk_diagnostic) on the same populations, within the diagnostics
-tolerance of the other GPU tests (1e-12 relative, 1e-15 absolute), on two
-calls in a row: the second call sees the first call's leftovers in the shared
-scratch and must not be affected by them. Enstrophy is not part of this entry
-point (it needs a velocity-field buffer).
+(their device memory all belongs to another runtime, such as an OpenACC data
+region, or to their own pool; cudaMalloc can fail on a full device and
+synchronises it). This entry point reduces caller-owned device populations
+with only a fixed file-scope device scratch array. Checked here:
 
+- against the CPU oracle's diagno / dissipation / strain-rate sums on the same
+  populations, and against the context entry point (bgk_diagnostic), within
+  the diagnostics tolerance of the other GPU tests (1e-12 relative, 1e-15
+  absolute), on calls in a row: each call sees the previous call's leftovers
+  in the shared scratch and must not be affected by them;
+- with caller rows padded (pitch_x > lx, the pad filled with NaN, which
+  would poison every sum it reached) on a non-default stream;
+- with no library context alive, device free memory is the same before and
+  after a call (after one warm-up call that loads the kernels).
+
+Enstrophy is not part of this entry point (it needs a velocity-field buffer).
 This file is named to be collected last.
 """
 import ctypes as C
@@ -21,27 +27,65 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 FIELDS = ["rho_mean", "ux_mean", "uy_mean", "uz_mean", "ke_mean", "t", "tke_norm", "diss", "tke", "eps_strain"]
+FORMS = {"fp64": "f64", "fp32": "f32", "fp16": "f16"}
+F16_SCALE = 2.0 ** 16
+SVISC, U0 = 0.005, 0.03
 
 
-def _device_copy(pops):
-    """The caller's own device copy of the populations (the caller allocates)."""
+def _device_copy(pops, pitch_x=None, pad_value=np.nan):
+    """The caller's own device copy of the populations (the caller allocates),
+    rows optionally padded to pitch_x with pad_value."""
     import torch
 
-    raw = np.ascontiguousarray(pops).view(np.uint8)
-    return torch.from_numpy(raw.copy()).cuda()
+    pops = np.ascontiguousarray(pops)
+    nz, ny, nx = pops.shape[1:]
+    px = pitch_x or nx
+    host = np.full((19, nz, ny, px), pad_value, dtype=pops.dtype)
+    host[..., :nx] = pops
+    raw = host.view(np.uint8).reshape(-1)
+    return torch.from_numpy(raw.copy()).cuda(), px
 
 
-def _noalloc(bgk, dev, shape, precision, box, mode, itime):
+def _noalloc(bgk, dev, shape, pitch_x, precision, omega, mode, itime, stream=None):
     lib = bgk.load()
     nx, ny, nz = shape
     per = dev.numel() // 19
     ptrs = (C.c_void_p * 19)(*[dev.data_ptr() + q * per for q in range(19)])
     d = bgk._abi.BgkDiag()
-    rc = lib.bgk_diagnostics_noalloc(ptrs, nx, ny, nz, nx, bgk._abi.PRECISIONS[precision], box.params.svisc,
-                                     box.omega, box.params.u0, box.scale if precision == "fp16" else 0.0,
-                                     bgk._abi.MODES[mode], itime, C.byref(d), None)
+    rc = lib.bgk_diagnostics_noalloc(ptrs, nx, ny, nz, pitch_x, bgk._abi.PRECISIONS[precision], SVISC, omega, U0,
+                                     F16_SCALE if precision == "fp16" else 0.0, bgk._abi.MODES[mode], itime,
+                                     C.byref(d), stream)
     assert rc == 0, lib.bgk_last_error()
     return d.as_dict()
+
+
+def _oracle_states(O, shape, precision, steps):
+    """Populations of a 3-component HIT field stepped by the oracle, with the
+    oracle's own diagnostics of each state."""
+    from bgk3d_hit_b200.hit import hit_velocity
+
+    nx, ny, nz = shape
+    u, v, w = hit_velocity((nz, ny, nx), k0=3, u_rms=U0, seed=77)
+    orc = O.OracleLattice(nx, ny, nz, form=FORMS[precision], scale=F16_SCALE)
+    orc.init_velocity(u, v, w, 1.0)
+    out, it = [], 0
+    for s in steps:
+        while it < s:
+            orc.step(SVISC, periodic=True)
+            it += 1
+        out.append((it, orc.get_pops(), orc.diagno(False), orc.diagno(True),
+                    orc.dissipation(SVISC, U0, it, False), orc.extras(SVISC)))
+    orc.close()
+    return out
+
+
+def _compare_oracle(got, itime, dg_c, dg_f, ds, ex, mode):
+    dg = dg_f if mode == "faithful" else dg_c
+    np.testing.assert_allclose([got[f] for f in FIELDS[:5]], dg, rtol=1e-12, atol=1e-15)
+    assert got["t"] == ds[0]
+    np.testing.assert_allclose([got["tke_norm"], got["diss"], got["tke"]], ds[1:], rtol=1e-12, atol=1e-15)
+    np.testing.assert_allclose(got["eps_strain"], ex[1], rtol=1e-12, atol=1e-18)
+    assert got["nonfinite"] == 0 and got["itime"] == itime
 
 
 def _compare(got, ref):
@@ -53,27 +97,92 @@ def _compare(got, ref):
 
 @pytest.mark.parametrize("precision", ["fp64", "fp32", "fp16"])
 @pytest.mark.parametrize("mode", ["corrected", "faithful"])
-def test_noalloc_matches_context_entry_point(bgk, precision, mode):
+def test_noalloc_matches_oracle_and_context_entry_point(bgk, oracle_mod, precision, mode):
     import torch
 
-    from bgk3d_hit_b200.hit import hit_velocity
-
     shape = (24, 20, 16)
-    u, v, w = hit_velocity(shape[::-1], k0=3, u_rms=0.03, seed=77)
-    box = bgk.BGK3D(*shape, svisc=0.005, u0=0.03, precision=precision, icheck=1, mode=mode)
-    box.init_velocity(u, v, w)
-    box.run(5)
-    ref5 = box.diagnostic(5)
-    dev5 = _device_copy(box.populations())
-    box.run(7)
-    ref12 = box.diagnostic(12)
-    dev12 = _device_copy(box.populations())
+    omega = oracle_mod.omega(SVISC, FORMS[precision])
+    states = _oracle_states(oracle_mod, shape, precision, (5, 12))
+    devs = [_device_copy(s[1])[0] for s in states]
     torch.cuda.synchronize()
-    # two calls in a row on different states, then the first state again
-    _compare(_noalloc(bgk, dev5, shape, precision, box, mode, 5), ref5)
-    _compare(_noalloc(bgk, dev12, shape, precision, box, mode, 12), ref12)
-    _compare(_noalloc(bgk, dev5, shape, precision, box, mode, 5), ref5)
-    box.close()
+    # calls in a row on different states, then the first state again
+    for k in (0, 1, 0):
+        it, _, dg_c, dg_f, ds, ex = states[k]
+        _compare_oracle(_noalloc(bgk, devs[k], shape, shape[0], precision, omega, mode, it), it, dg_c, dg_f, ds, ex,
+                        mode)
+    # the context entry point on the same populations
+    box = bgk.BGK3D(*shape, svisc=SVISC, u0=U0, precision=precision, icheck=1, mode=mode,
+                    fp16_scale=F16_SCALE if precision == "fp16" else 0.0)
+    try:
+        for k in (1, 0):
+            it, pops = states[k][:2]
+            box.set_populations(pops)
+            ref = box.diagnostic(it)
+            _compare(_noalloc(bgk, devs[k], shape, shape[0], precision, omega, mode, it), ref)
+    finally:
+        box.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32", "fp16"])
+def test_noalloc_padded_rows_on_a_caller_stream(bgk, oracle_mod, precision):
+    """Rows padded by 3 (and by 32) elements of NaN: a row pitch handled wrong
+    would read the pad and turn every sum non-finite, or shift the cells."""
+    import torch
+
+    shape = (21, 10, 9)
+    omega = oracle_mod.omega(SVISC, FORMS[precision])
+    (it, pops, dg_c, dg_f, ds, ex), = _oracle_states(oracle_mod, shape, precision, (3,))
+    stream = torch.cuda.Stream()
+    for pad in (3, 32):
+        dev, px = _device_copy(pops, pitch_x=shape[0] + pad)
+        stream.wait_stream(torch.cuda.current_stream())
+        for _ in range(2):
+            got = _noalloc(bgk, dev, shape, px, precision, omega, "corrected", it, stream=C.c_void_p(stream.cuda_stream))
+            _compare_oracle(got, it, dg_c, dg_f, ds, ex, "corrected")
+
+
+def test_noalloc_allocates_no_device_memory(bgk, oracle_mod):
+    """No library context is alive; one warm-up call loads the kernels (and
+    the scratch array with them); later calls leave the device's free memory
+    unchanged (cudaMemGetInfo, which sees any new device allocation of this
+    process at the driver's page granularity)."""
+    import gc
+
+    import torch
+
+    gc.collect()
+    shape = (64, 32, 24)
+    omega = oracle_mod.omega(SVISC, "f64")
+    (it, pops, dg_c, dg_f, ds, ex), = _oracle_states(oracle_mod, shape, "fp64", (2,))
+    dev, px = _device_copy(pops)
+    torch.cuda.synchronize()
+    _noalloc(bgk, dev, shape, px, "fp64", omega, "corrected", it)
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    for _ in range(3):
+        got = _noalloc(bgk, dev, shape, px, "fp64", omega, "corrected", it)
+    torch.cuda.synchronize()
+    free1 = torch.cuda.mem_get_info()[0]
+    assert free1 == free0
+    _compare_oracle(got, it, dg_c, dg_f, ds, ex, "corrected")
+
+
+def test_noalloc_reports_nonfinite_with_a_message(bgk, oracle_mod):
+    import torch
+
+    shape = (8, 6, 5)
+    (it, pops, *_), = _oracle_states(oracle_mod, shape, "fp64", (1,))
+    pops = pops.copy()
+    pops[3, 2, 1, 4] = np.nan
+    dev, px = _device_copy(pops)
+    torch.cuda.synchronize()
+    lib = bgk.load()
+    ptrs = (C.c_void_p * 19)(*[dev.data_ptr() + q * (dev.numel() // 19) for q in range(19)])
+    d = bgk._abi.BgkDiag()
+    rc = lib.bgk_diagnostics_noalloc(ptrs, *shape, px, 0, SVISC, 1.9, U0, 0.0, 0, it, C.byref(d), None)
+    assert rc == bgk._abi.BGK_ERR_NONFINITE
+    assert d.nonfinite == 1
+    assert b"1 cells with non-finite" in lib.bgk_last_error()
 
 
 def test_noalloc_rejects_oversized_and_invalid_boxes(bgk):

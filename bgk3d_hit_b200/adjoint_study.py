@@ -9,6 +9,10 @@ Loss = 0.5 mean |u(T) - u_tgt|^2. Reports, as one JSON object:
 - fd: the relative error of <grad, d> against central differences
   (L(u0 + h d) - L(u0 - h d)) / 2h over `dirs` seeded random unit directions d
   (max and median), and the same for tau;
+- fd_sweep: the same with a step chosen per direction by the usual h-sweep:
+  central differences at h = 1e-3 ... 1e-7 (`sweep` values), and the step
+  whose estimate agrees best with the next smaller step's (the plateau
+  between truncation error at large h and rounding noise at small h);
 - tangent: the relative difference between <grad, d> + grad_tau dtau and the
   tangent-linear derivative along (d, dtau) for a few directions;
 - cost: wall time of the adjoint call (forward with checkpoints, recomputation,
@@ -52,7 +56,7 @@ def _adj(box, u0, ut, T, K, grads):
 
 
 def run(size=128, steps=1000, ckpt=32, tau=0.51, k0=4.0, u_rms=0.03, dirs=64, h=1e-6, precision="fp64", ntan=4,
-        cache_gb=0.0, reps=5):
+        cache_gb=0.0, reps=5, sweep=(1e-3, 1e-4, 1e-5, 1e-6, 1e-7)):
     svisc = (tau - 0.5) / 3.0
     u0 = [np.ascontiguousarray(a) for a in hit_velocity(size, k0, u_rms, 1234)]
     ut = [np.ascontiguousarray(a) for a in hit_velocity(size, k0, u_rms, 4321)]
@@ -77,15 +81,25 @@ def run(size=128, steps=1000, ckpt=32, tau=0.51, k0=4.0, u_rms=0.03, dirs=64, h=
         ta.append(time.perf_counter() - t0)
     t_adj = float(np.median(ta))
     rng = np.random.default_rng(2024)
-    errs = []
+    errs, sweep_errs, sweep_h = [], [], []
+
+    def central(d, hh):
+        lp = _adj(box, [a + hh * b for a, b in zip(u0, d)], ut, steps, ckpt, False)[0]
+        lm = _adj(box, [a - hh * b for a, b in zip(u0, d)], ut, steps, ckpt, False)[0]
+        return (lp - lm) / (2 * hh)
+
     for _ in range(dirs):
         d = rng.standard_normal((3,) + u0[0].shape)
         d /= np.linalg.norm(d)
-        lp = _adj(box, [a + h * b for a, b in zip(u0, d)], ut, steps, ckpt, False)[0]
-        lm = _adj(box, [a - h * b for a, b in zip(u0, d)], ut, steps, ckpt, False)[0]
-        fd = (lp - lm) / (2 * h)
+        fd = central(d, h)
         ad = float(np.dot(g, d.reshape(-1)))
         errs.append(abs(ad - fd) / max(abs(fd), 1e-300))
+        if sweep:
+            est = [fd if hh == h else central(d, hh) for hh in sweep]
+            gaps = [abs(est[m] - est[m + 1]) for m in range(len(est) - 1)]
+            m = int(np.argmin(gaps))
+            sweep_h.append(sweep[m])
+            sweep_errs.append(abs(ad - est[m]) / max(abs(est[m]), 1e-300))
     # tau by central differences of boxes with omega = 1/(tau +- h)
     lt = []
     for s in (1, -1):
@@ -121,6 +135,9 @@ def run(size=128, steps=1000, ckpt=32, tau=0.51, k0=4.0, u_rms=0.03, dirs=64, h=
         "fd": {"max_rel_err": float(np.max(errs)), "median_rel_err": float(np.median(errs)),
                "p90_rel_err": float(np.percentile(errs, 90)),
                "tau_rel_err": abs(gtau - fd_tau) / abs(fd_tau)},
+        "fd_sweep": ({"max_rel_err": float(np.max(sweep_errs)), "median_rel_err": float(np.median(sweep_errs)),
+                      "p90_rel_err": float(np.percentile(sweep_errs, 90)),
+                      "h_chosen": {str(x): sweep_h.count(x) for x in sorted(set(sweep_h))}} if sweep_errs else None),
         "tangent": {"max_rel_err": float(np.max(tan_errs)), "directions": ntan},
         "cost": {"forward_s": t_fwd, "adjoint_s": t_adj, "adjoint_over_forward": t_adj / t_fwd},
         "vs_fp64": vs64,

@@ -7,6 +7,11 @@
 //             A = sum_p w_p lam_p (1 + P_p),
 //             B_a = 3 sum_p w_p lam_p c_pa (1 + 3 c_p.u) - 3 u_a sum_p w_p lam_p,
 //             and reverse streaming lam_t,q(x - c_q) = mu_q(x);
+// the adjoint buffers hold mu (the adjoint before its reverse streaming) at
+// the cell that formed it, and the next adjoint step gathers
+// lam_q(x) = mu_q(x + c_q): the forward's pull with the opposite shift, so
+// every store is the cell's own and the shifted accesses are loads, as in the
+// forward kernel;
 //   dL/domega = sum over steps and cells of -lam.(g - e);
 //   tangent   df_p = (1 - omega) dg_p + omega de_p + (e_p - g_p) domega,
 //             de_p = w_p [(1 + P_p) drho + rho (3 (c_p.du)(1 + 3 c_p.u) - 3 u.du)],
@@ -74,7 +79,10 @@ __global__ void __launch_bounds__(DIAG_THREADS) k_adj_terminal(Pops<const typena
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
       const double l = r * (d[0] * (cxq(q) - u[0]) + d[1] * (cyq(q) - u[1]) + d[2] * (czq(q) - u[2]));
-      lam.p[q][o] = (S)l;
+      // in the adjoint buffers' convention: lam_q(y) sits at y + c_q
+      const long long oq = wrapa(i + cxq(q), g.nx) +
+                           (long long)g.sx * (wrapa(j + cyq(q), g.ny) + (long long)g.ny * wrapa(k + czq(q), g.nz));
+      lam.p[q][oq] = (S)l;
     }
   }
   acc_block(loss, sh, acc);
@@ -87,9 +95,12 @@ __global__ void __launch_bounds__(DIAG_THREADS) k_adj_terminal(Pops<const typena
 //   A = L0 (1 + a) + 3 u.M1 + 4.5 u.M2.u,    a = -1.5 |u|^2,
 //   B = 3 (M1 + 3 M2 u - u L0),
 //   sum lam.(e - g) = rho A - L0 - S1.
-// So no population array stays live across the cell. lam is read again from
-// cache for the output. rho and u are formed in the form's arithmetic R, the
-// moment sums and A, B, G in double. Each block adds its dL/domega
+// So no population array stays live across the cell. The forward state is
+// pulled from x - c_q and lam gathered from x + c_q (lam_q(x) = mu_q(x + c_q)
+// of the previous adjoint step), both as row loads like the forward kernel's;
+// lam is read again from cache for the output, mu_q(x), stored at the cell.
+// rho and u are formed in the form's arithmetic R, the moment sums and A, B,
+// G in double. Each block adds its dL/domega
 // contribution (warp shuffles, then the four warp sums in order) into its
 // own compensated pair acc[2*block].
 template <class F>
@@ -107,18 +118,20 @@ __global__ void __launch_bounds__(128, 4) k_adj_step(Pops<const typename F::S> f
     const int jm = j == 0 ? g.ny - 1 : j - 1, jp = j == g.ny - 1 ? 0 : j + 1;
     const int km = k == 0 ? g.nz - 1 : k - 1, kp = k == g.nz - 1 ? 0 : k + 1;
     const int o = i + g.sx * (j + g.ny * k);
-    auto offq = [&](int q) {
-      const int ii = cxq(q) > 0 ? im : (cxq(q) < 0 ? ip : i);
-      const int jj = cyq(q) > 0 ? jm : (cyq(q) < 0 ? jp : j);
-      const int kk = czq(q) > 0 ? km : (czq(q) < 0 ? kp : k);
+    // s = +1: x - c_q (pull of the state); s = -1: x + c_q (gather of lam)
+    auto offq = [&](int q, int s) {
+      const int cx = s * cxq(q), cy = s * cyq(q), cz = s * czq(q);
+      const int ii = cx > 0 ? im : (cx < 0 ? ip : i);
+      const int jj = cy > 0 ? jm : (cy < 0 ? jp : j);
+      const int kk = cz > 0 ? km : (cz < 0 ? kp : k);
       return ii + g.sx * (jj + g.ny * kk);
     };
     R rho = (R)1, jx = 0, jy = 0, jz = 0;
     double L0 = 0, m1x = 0, m1y = 0, m1z = 0, mxx = 0, myy = 0, mzz = 0, mxy = 0, mxz = 0, myz = 0, S1 = 0;
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
-      const R x = (R)__ldg(ft.p[q] + offq(q));
-      const double lam = (double)__ldg(lin.p[q] + o);
+      const R x = (R)__ldg(ft.p[q] + offq(q, 1));
+      const double lam = (double)__ldg(lin.p[q] + offq(q, -1));
       rho += x;
       jx += (R)cxq(q) * x;
       jy += (R)cyq(q) * x;
@@ -152,10 +165,10 @@ __global__ void __launch_bounds__(128, 4) k_adj_step(Pops<const typename F::S> f
     const R om = omega;
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
-      const R lam = (R)__ldg(lin.p[q] + o);
+      const R lam = (R)__ldg(lin.p[q] + offq(q, -1));
       const R gq = (R)(G + cdot<double>(q, Bx, By, Bz));
       const R mu = om1 * lam + om * gq;
-      lout.p[q][offq(q)] = (S)mu;  // reverse streaming: lam_t,q(x - c_q) = mu_q(x)
+      lout.p[q][o] = (S)mu;  // mu_q(x): cell x - c_q of the next adjoint step gathers it as its lam_q
     }
   }
   // fixed-order block sum into this block's running pair
@@ -180,12 +193,13 @@ __global__ void __launch_bounds__(DIAG_THREADS) k_adj_grad_u0(Pops<const typenam
   const long long n = (long long)g.nx * g.ny * g.nz;
   for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
     const int i = (int)(c % g.nx), j = (int)((c / g.nx) % g.ny), k = (int)(c / ((long long)g.nx * g.ny));
-    const long long o = i + (long long)g.sx * (j + (long long)g.ny * k);
     const double ux = u0[c], uy = u0[n + c], uz = u0[2 * n + c];
     double L0 = 0, Lx = 0, Ly = 0, Lz = 0;
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
-      const double wl = wq<double>(q) * (double)lam.p[q][o];
+      const long long oq = wrapa(i + cxq(q), g.nx) +
+                           (long long)g.sx * (wrapa(j + cyq(q), g.ny) + (long long)g.ny * wrapa(k + czq(q), g.nz));
+      const double wl = wq<double>(q) * (double)lam.p[q][oq];  // lam_q(y) = mu_q(y + c_q)
       const double t = wl * (1.0 + 3.0 * cdot<double>(q, ux, uy, uz));
       L0 += wl;
       Lx += t * cxq(q);

@@ -36,18 +36,34 @@ FORMS = ("fp64", "fp32", "fp16")
 
 
 def run(size=512, steps=5000, every=100, k0=6.0, tau=0.503, u_rms=0.03, seed=1234, scheme="two_lattice",
-        forms=FORMS, device=0, les_cs=0.0):
+        forms=FORMS, device=0, les_cs=0.0, device_ic=None):
+    """device_ic: make the initial field on the GPU (hit_velocity_device) and
+    initialise from device memory; default for boxes of 512^3 cells and more."""
     svisc = (tau - 0.5) / 3.0
+    if device_ic is None:
+        device_ic = size ** 3 >= 512 ** 3
     t0 = time.time()
-    u, v, w = hit_velocity(size, k0, u_rms, seed)
+    if device_ic:
+        from .hit import hit_velocity_device
+
+        u, v, w = hit_velocity_device(size, k0, u_rms, seed, device=device)
+    else:
+        u, v, w = hit_velocity(size, k0, u_rms, seed)
     t_ic = time.time() - t0
     boxes = {}
     for f in forms:
         b = BGK3D(size, svisc=svisc, u0=u_rms, precision=f, scheme=scheme, icheck=every, device=device,
                   les_cs=les_cs)
-        b.init_velocity(u, v, w)
+        if device_ic:
+            b.init_velocity_device(u, v, w)
+        else:
+            b.init_velocity(u, v, w)
         boxes[f] = b
     del u, v, w
+    if device_ic:
+        import torch
+
+        torch.cuda.empty_cache()
     series = {f: {"step": [], "E": [], "eps": [], "diss": [], "rho": []} for f in forms}
     blowup = {f: None for f in forms}
     spec = {}

@@ -170,3 +170,38 @@ def test_init_velocity_device_equals_host_init(bgk, form, scheme):
     finally:
         a.close()
         b.close()
+
+
+def test_faithful_mode_dissipation_is_the_periodic_value(bgk, oracle_mod):
+    """The reference computes dissipation after col_MC's pointer swap
+    (SRC/col_MC.F90:364-421, SRC/dissipation.F90:76-94), so its border cells
+    pull ghost values of the lattice that were filled two steps earlier, or
+    never (the second lattice's ghosts before its first boundaries call). The
+    GPU has no ghosts and computes the periodic value in both modes: here, on
+    the C1 box (TGV 64^3, faithful init, nu = 0.01), it equals the oracle's
+    periodic dissipation to 1e-12 while the oracle's stale-ghost (faithful)
+    value differs from it by 64x at step 1, ~1% at step 2, ~0.5% at step 10
+    and ~3e-5 at step 100 (asserted as ranges)."""
+    orc = oracle_mod.OracleLattice(64, 64, 64, form="f64")
+    orc.init_tgv(0.05, faithful=True)
+    box = bgk.BGK3D(64, svisc=0.01, u0=0.05, precision="fp64", icheck=1, mode="faithful")
+    box.set_populations(orc.get_pops())
+    gaps = {}
+    try:
+        for it in range(1, 101):
+            orc.step(0.01)  # boundaries (ghost fill) + col_MC, as the reference loop
+            box.boundaries(it)
+            box.col_MC(it)
+            if it in (1, 2, 10, 100):
+                d = box.diagnostic(it)
+                per = orc.dissipation(0.01, 0.05, it, False)
+                stale = orc.dissipation(0.01, 0.05, it, True)
+                assert d["diss"] == pytest.approx(per[2], rel=1e-12)
+                assert d["tke_norm"] == pytest.approx(per[1], rel=1e-12)
+                gaps[it] = abs(stale[2] - per[2]) / abs(per[2])
+    finally:
+        orc.close()
+        box.close()
+    assert gaps[1] > 10
+    assert 1e-3 < gaps[2] < 1e-1 and 1e-3 < gaps[10] < 1e-1
+    assert 1e-6 < gaps[100] < 1e-3

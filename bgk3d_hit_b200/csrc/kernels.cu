@@ -11,6 +11,8 @@
 //                per-block partials
 //   k_enstrophy  0.5|curl u|^2 from the local velocity field
 //   k_shift3     shift-only stencil of SRC/do_somethingGPU.F90:37-100
+#include <cstdlib>
+
 #include "kernels.h"
 #include "reduce.cuh"
 
@@ -472,14 +474,43 @@ __global__ void __launch_bounds__(256, 5) k_aa_f16_odd(Pops<__half> a, Geo g, St
 // blocks, 63.4 with the odd step capped at 80 registers (282 spilled bytes),
 // 62.8-65.0 with two cells per thread on the odd step, and 58 for one cell per
 // thread. The LES odd step keeps its addresses (4 blocks).
-template <bool ODD, bool LES>
+__device__ __forceinline__ void prefetch_l2(const void* p, unsigned bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
+// Rows of the block `ahead` blocks after this one (grid order): lanes 0..18
+// of each warp ask the L2 for one population's 256-byte segment of that
+// warp's rows (tpr >= 32 only, so a warp covers one row segment).
+template <bool ODD>
+__device__ __forceinline__ void prefetch_rows_ahead(const Pops<__half>& a, const Geo& g, int log_tpr, int ahead) {
+  const int lane = threadIdx.x & 31;
+  if (ahead <= 0 || log_tpr < 5 || lane >= Q) return;
+  const long long nb = (long long)gridDim.x * gridDim.y;
+  const long long b = blockIdx.x + (long long)gridDim.x * blockIdx.y + ahead;
+  if (b >= nb) return;
+  const int bx = (int)(b % gridDim.x), k = (int)(b / gridDim.x);
+  const int t = bx * blockDim.x + (threadIdx.x & ~31);
+  const int j = t >> log_tpr, i0 = (t & ((1 << log_tpr) - 1)) * 4;
+  if (j >= g.ny) return;
+  const int q = lane;
+  int jj = j, kk = k;
+  if (ODD) {
+    jj = wrapi(j - cyq(q), g.ny);
+    kk = wrapi(k - czq(q), g.nz);
+  }
+  const __half* p = a.p[ODD ? oppq(q) : q] + g.sx * (jj + g.ny * kk) + i0;
+  prefetch_l2(p, 256);
+}
+
+template <bool ODD, bool LES, int VAR = 0>
 __global__ void __launch_bounds__(128, ODD ? (LES ? 4 : 5) : 6) k_aa_f16v(Pops<__half> a, Geo g, StepK K,
-                                                                          int log_tpr) {
+                                                                          int log_tpr, int ahead = 0) {
   const int tpr = 1 << log_tpr;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = t >> log_tpr, pos = t & (tpr - 1);
   const int k = blockIdx.y;
   if (j >= g.ny) return;  // whole warps: ny*tpr is a multiple of 32
+  if (VAR & 2) prefetch_rows_ahead<ODD>(a, g, log_tpr, ahead);
   const XLanes xl(tpr, pos, threadIdx.x & 31);
   const int i0 = pos * 4;
   const int jm = j == 0 ? g.ny - 1 : j - 1, jp = j == g.ny - 1 ? 0 : j + 1;
@@ -492,13 +523,41 @@ __global__ void __launch_bounds__(128, ODD ? (LES ? 4 : 5) : 6) k_aa_f16v(Pops<_
     return g.sx * (jj + g.ny * kk);
   };
   uint2 Y[Q];
+  if (ODD && (VAR & 1)) {
+    // every row load and crossing-element load issued before any shuffle
+    unsigned short E[Q];
 #pragma unroll
-  for (int q = 0; q < Q; ++q) {
-    if (!ODD) {
-      Y[q] = __ldg(reinterpret_cast<const uint2*>(a.p[q] + row(0, 0) + i0));
-    } else {
+    for (int q = 0; q < Q; ++q) {
       const __half* p = a.p[oppq(q)] + row(-cyq(q), -czq(q));
-      Y[q] = shift_in(__ldg(reinterpret_cast<const uint2*>(p + i0)), cxq(q), p, i_prev, i_next, xl);
+      Y[q] = __ldg(reinterpret_cast<const uint2*>(p + i0));
+      E[q] = 0;
+      if (cxq(q) > 0 && xl.edge_prev) E[q] = ldg_u16(p + i_prev);
+      if (cxq(q) < 0 && xl.edge_next) E[q] = ldg_u16(p + i_next);
+    }
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      const uint2 A = Y[q];
+      if (cxq(q) > 0) {
+        unsigned prev = __shfl_sync(0xffffffffu, A.y >> 16, xl.src_prev);
+        if (xl.edge_prev) prev = E[q];
+        Y[q].x = __byte_perm(A.x, prev, 0x1054);
+        Y[q].y = __byte_perm(A.x, A.y, 0x5432);
+      } else if (cxq(q) < 0) {
+        unsigned next = __shfl_sync(0xffffffffu, A.x & 0xffffu, xl.src_next);
+        if (xl.edge_next) next = E[q];
+        Y[q].x = __byte_perm(A.x, A.y, 0x5432);
+        Y[q].y = __byte_perm(A.y, next, 0x5432);
+      }
+    }
+  } else {
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      if (!ODD) {
+        Y[q] = __ldg(reinterpret_cast<const uint2*>(a.p[q] + row(0, 0) + i0));
+      } else {
+        const __half* p = a.p[oppq(q)] + row(-cyq(q), -czq(q));
+        Y[q] = shift_in(__ldg(reinterpret_cast<const uint2*>(p + i0)), cxq(q), p, i_prev, i_next, xl);
+      }
     }
   }
   if constexpr (LES) collide4_f16_les(Y, K);
@@ -1101,8 +1160,34 @@ static cudaError_t aa_impl(const Lattice& a, int odd, const StepK& K, int varian
   // FP16: four cells per thread where the box fits it (automatic or 4)
   if (lt4 >= 0) {
     const dim3 grid = f16v_grid(a.g, lt4, a.g.nz);
-    if (odd) k_aa_f16v<true, false><<<grid, 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
-    else k_aa_f16v<false, false><<<grid, 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
+    static int var = -1, mult = 1;
+    if (var < 0) {
+      const char* e = getenv("BGK_AA_VARIANT");
+      var = e ? atoi(e) : 0;
+      const char* m = getenv("BGK_AA_AHEAD");
+      mult = m ? atoi(m) : 1;
+    }
+    int ahead = 0;
+    if (var & 6) {
+      int dev = 0, nsm = 148, bps = 1;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+      if (odd) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_aa_f16v<true, false, 3>, 128, 0);
+      else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_aa_f16v<false, false, 2>, 128, 0);
+      ahead = nsm * bps * mult;
+    }
+    auto P = pops_of<__half>(a);
+    if (odd) {
+      switch (var & 3) {
+        case 0: k_aa_f16v<true, false, 0><<<grid, 128, 0, st>>>(P, a.g, K, lt4, 0); break;
+        case 1: k_aa_f16v<true, false, 1><<<grid, 128, 0, st>>>(P, a.g, K, lt4, 0); break;
+        case 2: k_aa_f16v<true, false, 2><<<grid, 128, 0, st>>>(P, a.g, K, lt4, ahead); break;
+        case 3: k_aa_f16v<true, false, 3><<<grid, 128, 0, st>>>(P, a.g, K, lt4, ahead); break;
+      }
+    } else {
+      if (var & 4) k_aa_f16v<false, false, 2><<<grid, 128, 0, st>>>(P, a.g, K, lt4, ahead);
+      else k_aa_f16v<false, false, 0><<<grid, 128, 0, st>>>(P, a.g, K, lt4, 0);
+    }
     return cudaGetLastError();
   }
   if (odd && F::id == FORM_F16)

@@ -105,11 +105,14 @@ __device__ __forceinline__ float2 u2f2(unsigned u) { return __half22float2(*rein
 // Collision of four FP16 cells packed in Y (population q of cell m in half m
 // of Y[q]), F16::cell's arithmetic, on cells 0, 1 (low words) then cells 2, 3
 // (high words): each half's outputs replace its inputs in Y, so only two
-// cells' moments are live at a time.
+// cells' moments are live at a time. LES: the Smagorinsky collision
+// (moments16_les: per-cell relaxation constants, the same pair update).
+template <bool LES>
 __device__ __forceinline__ void collide4_f16(uint2 (&Y)[Q], const StepK& K) {
 #pragma unroll
   for (int h = 0; h < 2; ++h) {
     Mom16 M[2];
+    float om1[2] = {K.om1, K.om1};
 #pragma unroll
     for (int m = 0; m < 2; ++m) {
       float y[Q];
@@ -118,95 +121,25 @@ __device__ __forceinline__ void collide4_f16(uint2 (&Y)[Q], const StepK& K) {
         const float2 f = u2f2(h ? Y[q].y : Y[q].x);
         y[q] = m ? f.y : f.x;
       }
-      M[m] = moments16(y, K);
+      if constexpr (LES) M[m] = moments16_les(y, K, om1[m]);
+      else M[m] = moments16(y, K);
     }
 #pragma unroll
     for (int q = 0; q < 9; ++q) {
       const int r = oppq(q);
       const float2 a = u2f2(h ? Y[q].y : Y[q].x), c = u2f2(h ? Y[r].y : Y[r].x);
       float p0, p1, o0, o1;
-      pair16(q, a.x, c.x, M[0], K.om1, p0, o0);
-      pair16(q, a.y, c.y, M[1], K.om1, p1, o1);
+      pair16(q, a.x, c.x, M[0], om1[0], p0, o0);
+      pair16(q, a.y, c.y, M[1], om1[1], p1, o1);
       const unsigned pq = h2u(__floats2half2_rn(p0, p1)), pr = h2u(__floats2half2_rn(o0, o1));
       if (h) { Y[q].y = pq; Y[r].y = pr; } else { Y[q].x = pq; Y[r].x = pr; }
     }
     {
       const float2 a = u2f2(h ? Y[Q - 1].y : Y[Q - 1].x);
-      const unsigned pz = h2u(__floats2half2_rn(rest16(a.x, M[0], K.om1), rest16(a.y, M[1], K.om1)));
+      const unsigned pz = h2u(__floats2half2_rn(rest16(a.x, M[0], om1[0]), rest16(a.y, M[1], om1[1])));
       if (h) Y[Q - 1].y = pz; else Y[Q - 1].x = pz;
     }
   }
-}
-
-// The Smagorinsky collision of the FP16 form (lattice.cuh cell16_les) on four
-// cells packed in Y, one cell at a time so that no per-population array but
-// the cell's 19 inputs stays live: the Pi_neq sums are accumulated in the
-// order of cell16_les's expressions while the terms are formed, and the
-// equilibrium terms t_q are formed again for the output (the same operations,
-// so the same values). The output replaces the cell's half of Y.
-__device__ __forceinline__ void les16_cell(uint2 (&Y)[Q], int m, const StepK& k) {
-  float y[Q];
-#pragma unroll
-  for (int q = 0; q < Q; ++q) {
-    const float2 f = u2f2(m < 2 ? Y[q].x : Y[q].y);
-    y[q] = (m & 1) ? f.y : f.x;
-  }
-  const Mom16 M = moments16(y, k);
-  const float dr = M.dr;
-  auto tq = [&](int q) {
-    const float cu = cdotu(q, M);
-    const float P = __fmaf_rn(3.0f, cu, __fmaf_rn(__fmul_rn(4.5f, cu), cu, M.a));
-    return __fmaf_rn(dr, P, __fadd_rn(dr, P));
-  };
-  auto wf = [](int q) { return wclass(q) == 0 ? 1.0f / 3.0f : (wclass(q) == 1 ? 1.0f / 18.0f : 1.0f / 36.0f); };
-  float Pxx = 0.0f, Pyy = 0.0f, Pzz = 0.0f, Pxz = 0.0f, Pxy = 0.0f, Pyz = 0.0f;
-#pragma unroll
-  for (int q = 0; q < Q - 1; ++q) {
-    const float nn = __fsub_rn(__fmul_rn(y[q], k.inv), __fmul_rn(wf(q), tq(q)));
-    // Pxx = n0 + n1 + n2 + n3 + n4 + n9 + n10 + n11 + n12 + n13
-    if (q == 0) Pxx = nn;
-    else if (q <= 4 || (q >= 9 && q <= 13)) Pxx = Pxx + nn;
-    // Pyy = n0 + n2 + n6 + n7 + n8 + n9 + n11 + n15 + n16 + n17
-    if (q == 0) Pyy = nn;
-    else if (q == 2 || (q >= 6 && q <= 9) || q == 11 || q >= 15) Pyy = Pyy + nn;
-    // Pzz = n1 + n3 + n5 + n6 + n8 + n10 + n12 + n14 + n15 + n17
-    if (q == 1) Pzz = nn;
-    else if (q == 3 || q == 5 || q == 6 || q == 8 || q == 10 || q == 12 || q == 14 || q == 15 || q == 17) Pzz = Pzz + nn;
-    // Pxz = -n1 + n3 + n10 - n12
-    if (q == 1) Pxz = -nn;
-    else if (q == 3 || q == 10) Pxz = Pxz + nn;
-    else if (q == 12) Pxz = Pxz - nn;
-    // Pxy = -n0 + n2 + n9 - n11
-    if (q == 0) Pxy = -nn;
-    else if (q == 2 || q == 9) Pxy = Pxy + nn;
-    else if (q == 11) Pxy = Pxy - nn;
-    // Pyz = n6 - n8 + n15 - n17
-    if (q == 6) Pyz = nn;
-    else if (q == 15) Pyz = Pyz + nn;
-    else if (q == 8 || q == 17) Pyz = Pyz - nn;
-  }
-  float pt = __fmul_rn(Pxx, Pxx);
-  pt = __fmaf_rn(Pyy, Pyy, pt);
-  pt = __fmaf_rn(Pzz, Pzz, pt);
-  pt = __fmaf_rn(2.0f * Pxy, Pxy, pt);
-  pt = __fmaf_rn(2.0f * Pxz, Pxz, pt);
-  pt = __fmaf_rn(2.0f * Pyz, Pyz, pt);
-  const float tau = __fadd_rn(k.tauh_f, __fmul_rn(0.5f, __fsqrt_rn(__fmaf_rn(k.cs18_f, __fsqrt_rn(pt), k.tau2_f))));
-  const float om = __fdiv_rn(1.0f, tau);
-  const float om1 = __fsub_rn(1.0f, om);
-  const float oms = __fmul_rn(om, k.scale);
-#pragma unroll
-  for (int q = 0; q < Q; ++q) {
-    const unsigned short h =
-        __half_as_ushort(__float2half_rn(__fmaf_rn(__fmul_rn(oms, wf(q)), tq(q), __fmul_rn(om1, y[q]))));
-    unsigned& word = m < 2 ? Y[q].x : Y[q].y;
-    word = (m & 1) ? ((word & 0xffffu) | ((unsigned)h << 16)) : ((word & 0xffff0000u) | h);
-  }
-}
-
-__device__ __forceinline__ void collide4_f16_les(uint2 (&Y)[Q], const StepK& K) {
-#pragma unroll
-  for (int m = 0; m < 4; ++m) les16_cell(Y, m, K);
 }
 
 // Lanes that exchange x-neighbours in the four-cells-per-thread FP16 kernels:
@@ -329,8 +262,7 @@ __global__ void __launch_bounds__(128, 6) k_two_f16v(Pops<const __half> src, Pop
       Y[q].y = __byte_perm(A.y, next, 0x5432);
     }
   }
-  if constexpr (LES) collide4_f16_les(Y, K);
-  else collide4_f16(Y, K);
+  collide4_f16<LES>(Y, K);
   const int o = i0 + g.sx * (j + g.ny * k);
 #pragma unroll
   for (int q = 0; q < Q; ++q) *reinterpret_cast<uint2*>(dst.p[q] + o) = Y[q];
@@ -473,7 +405,8 @@ __global__ void __launch_bounds__(256, 5) k_aa_f16_odd(Pops<__half> a, Geo g, St
 // with the addresses kept (128 registers, 4 blocks), 69.5 with 256-thread
 // blocks, 63.4 with the odd step capped at 80 registers (282 spilled bytes),
 // 62.8-65.0 with two cells per thread on the odd step, and 58 for one cell per
-// thread. The LES odd step keeps its addresses (4 blocks).
+// thread. The LES odd step recomputes its store rows the same way (96 registers,
+// a few spilled bytes, 5 blocks per SM).
 __device__ __forceinline__ void prefetch_l2(const void* p, unsigned bytes) {
   asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
 }
@@ -503,7 +436,7 @@ __device__ __forceinline__ void prefetch_rows_ahead(const Pops<__half>& a, const
 }
 
 template <bool ODD, bool LES, int VAR = 0>
-__global__ void __launch_bounds__(128, ODD ? (LES ? 4 : 5) : 6) k_aa_f16v(Pops<__half> a, Geo g, StepK K,
+__global__ void __launch_bounds__(128, ODD ? 5 : 6) k_aa_f16v(Pops<__half> a, Geo g, StepK K,
                                                                           int log_tpr, int ahead = 0) {
   const int tpr = 1 << log_tpr;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -560,10 +493,9 @@ __global__ void __launch_bounds__(128, ODD ? (LES ? 4 : 5) : 6) k_aa_f16v(Pops<_
       }
     }
   }
-  if constexpr (LES) collide4_f16_les(Y, K);
-  else collide4_f16(Y, K);
+  collide4_f16<LES>(Y, K);
   int js = j, ks = k;  // store rows: recomputed after the collision (BGK odd step)
-  if (ODD && !LES) asm volatile("" : "+r"(js), "+r"(ks));
+  if (ODD) asm volatile("" : "+r"(js), "+r"(ks));
   const int jms = js == 0 ? g.ny - 1 : js - 1, jps = js == g.ny - 1 ? 0 : js + 1;
   const int kms = ks == 0 ? g.nz - 1 : ks - 1, kps = ks == g.nz - 1 ? 0 : ks + 1;
   auto row_out = [&](int dy, int dz) {

@@ -215,28 +215,43 @@ __device__ __forceinline__ float rest16(float y, const Mom16& m, float om1) {
   return __fmaf_rn(om1, y, m.kra[0]);
 }
 
-// FP16 form with the Smagorinsky closure: per cell, Pi_neq from the
-// non-equilibrium n_q = y_q/scale - w_q (dr + (1 + dr) P_q), Ptotal =
-// sqrt(Pi:Pi), tau = tauh + sqrt(cs18 Ptotal + tau2)/2 and the relaxation
-// y' = (1 - omega_eff) y + omega_eff scale w (dr + (1 + dr) P).
-__device__ __forceinline__ void cell16_les(const float (&y)[Q], __half (&s)[Q], const StepK& k) {
-  const Mom16 m = moments16(y, k);
-  const float dr = m.dr;
-  float t[Q], nn[Q];
-#pragma unroll
-  for (int q = 0; q < Q; ++q) {
-    const float cu = cdotu(q, m);
-    const float P = __fmaf_rn(3.0f, cu, __fmaf_rn(__fmul_rn(4.5f, cu), cu, m.a));
-    t[q] = __fmaf_rn(dr, P, __fadd_rn(dr, P));
-    const float w = wclass(q) == 0 ? 1.0f / 3.0f : (wclass(q) == 1 ? 1.0f / 18.0f : 1.0f / 36.0f);
-    nn[q] = __fsub_rn(__fmul_rn(y[q], k.inv), __fmul_rn(w, t[q]));
-  }
-  const float Pxx = nn[0] + nn[1] + nn[2] + nn[3] + nn[4] + nn[9] + nn[10] + nn[11] + nn[12] + nn[13];
-  const float Pyy = nn[0] + nn[2] + nn[6] + nn[7] + nn[8] + nn[9] + nn[11] + nn[15] + nn[16] + nn[17];
-  const float Pzz = nn[1] + nn[3] + nn[5] + nn[6] + nn[8] + nn[10] + nn[12] + nn[14] + nn[15] + nn[17];
-  const float Pxz = -nn[1] + nn[3] + nn[10] - nn[12];
-  const float Pxy = -nn[0] + nn[2] + nn[9] - nn[11];
-  const float Pyz = nn[6] - nn[8] + nn[15] - nn[17];
+// FP16 form with the Smagorinsky closure: the sums, dr, u and a of
+// moments16; Pi_neq from the second moments of the stored values minus the
+// equilibrium's closed form (D3Q19: sum_q c_a c_b (f_eq - w)_q =
+// dr delta_ab / 3 + rho u_a u_b, rho = 1 + dr), Ptotal = sqrt(Pi:Pi),
+// tau = tauh + sqrt(cs18 Ptotal + tau2)/2, omega_eff = 1/tau; the returned
+// moments carry K = omega_eff scale w per weight class, so pair16 / rest16
+// with om1 = 1 - omega_eff give the relaxation. Oracle: fast16_les_cell.
+__device__ __forceinline__ Mom16 moments16_les(const float (&y)[Q], const StepK& k, float& om1) {
+  const float sp = __fadd_rn(__fadd_rn(__fadd_rn(y[0], y[1]), __fadd_rn(y[2], y[3])), y[4]);
+  const float sm = __fadd_rn(__fadd_rn(__fadd_rn(y[9], y[10]), __fadd_rn(y[11], y[12])), y[13]);
+  const float s0 = __fadd_rn(__fadd_rn(__fadd_rn(__fadd_rn(y[5], y[6]), __fadd_rn(y[7], y[8])),
+                                       __fadd_rn(__fadd_rn(y[14], y[15]), __fadd_rn(y[16], y[17]))),
+                             y[18]);
+  const float sum = __fadd_rn(__fadd_rn(sp, sm), s0);
+  const float jx = __fsub_rn(sp, sm);
+  const float jyp = __fadd_rn(__fadd_rn(__fadd_rn(y[2], y[6]), __fadd_rn(y[7], y[8])), y[11]);
+  const float jym = __fadd_rn(__fadd_rn(__fadd_rn(y[0], y[9]), __fadd_rn(y[15], y[16])), y[17]);
+  const float jzp = __fadd_rn(__fadd_rn(__fadd_rn(y[3], y[5]), __fadd_rn(y[6], y[12])), y[17]);
+  const float jzm = __fadd_rn(__fadd_rn(__fadd_rn(y[1], y[8]), __fadd_rn(y[10], y[14])), y[15]);
+  Mom16 m;
+  const float dr = __fmul_rn(sum, k.inv);
+  m.dr = dr;
+  const float rp = __fadd_rn(1.0f, dr);
+  const float r = __fmul_rn(k.inv, __frcp_rn(rp));  // = inv/(1 + dr), inv a power of two
+  m.ux = __fmul_rn(jx, r);
+  m.uy = __fmul_rn(__fsub_rn(jyp, jym), r);
+  m.uz = __fmul_rn(__fsub_rn(jzp, jzm), r);
+  const float usq = __fmaf_rn(m.uz, m.uz, __fmaf_rn(m.uy, m.uy, __fmul_rn(m.ux, m.ux)));
+  m.a = __fmul_rn(-1.5f, usq);
+  const float d3 = __fmul_rn(dr, 1.0f / 3.0f);
+  const float rux = __fmul_rn(rp, m.ux), ruy = __fmul_rn(rp, m.uy);
+  const float Pxx = __fmaf_rn(__fadd_rn(sp, sm), k.inv, -__fmaf_rn(rux, m.ux, d3));
+  const float Pyy = __fmaf_rn(__fadd_rn(jyp, jym), k.inv, -__fmaf_rn(ruy, m.uy, d3));
+  const float Pzz = __fmaf_rn(__fadd_rn(jzp, jzm), k.inv, -__fmaf_rn(__fmul_rn(rp, m.uz), m.uz, d3));
+  const float Pxy = __fmaf_rn(__fsub_rn(__fadd_rn(y[2], y[9]), __fadd_rn(y[0], y[11])), k.inv, -__fmul_rn(rux, m.uy));
+  const float Pxz = __fmaf_rn(__fsub_rn(__fadd_rn(y[3], y[10]), __fadd_rn(y[1], y[12])), k.inv, -__fmul_rn(rux, m.uz));
+  const float Pyz = __fmaf_rn(__fsub_rn(__fadd_rn(y[6], y[15]), __fadd_rn(y[8], y[17])), k.inv, -__fmul_rn(ruy, m.uz));
   float pt = __fmul_rn(Pxx, Pxx);
   pt = __fmaf_rn(Pyy, Pyy, pt);
   pt = __fmaf_rn(Pzz, Pzz, pt);
@@ -245,12 +260,31 @@ __device__ __forceinline__ void cell16_les(const float (&y)[Q], __half (&s)[Q], 
   pt = __fmaf_rn(2.0f * Pyz, Pyz, pt);
   const float tau = __fadd_rn(k.tauh_f, __fmul_rn(0.5f, __fsqrt_rn(__fmaf_rn(k.cs18_f, __fsqrt_rn(pt), k.tau2_f))));
   const float om = __fdiv_rn(1.0f, tau);
-  const float om1 = __fsub_rn(1.0f, om);
+  om1 = __fsub_rn(1.0f, om);
+  const float oms = __fmul_rn(om, k.scale);
 #pragma unroll
-  for (int q = 0; q < Q; ++q) {
-    const float w = wclass(q) == 0 ? 1.0f / 3.0f : (wclass(q) == 1 ? 1.0f / 18.0f : 1.0f / 36.0f);
-    s[q] = __float2half_rn(__fmaf_rn(__fmul_rn(__fmul_rn(om, k.scale), w), t[q], __fmul_rn(om1, y[q])));
+  for (int c = 0; c < 3; ++c) {
+    const float K = __fmul_rn(oms, c == 0 ? 1.0f / 3.0f : (c == 1 ? 1.0f / 18.0f : 1.0f / 36.0f));
+    const float kd = __fmul_rn(K, dr);
+    const float kr = __fadd_rn(K, kd);
+    m.kr3[c] = __fmul_rn(3.0f, kr);
+    m.kr45[c] = __fmul_rn(4.5f, kr);
+    m.kra[c] = __fmaf_rn(kr, m.a, kd);
   }
+  return m;
+}
+
+__device__ __forceinline__ void cell16_les(const float (&y)[Q], __half (&s)[Q], const StepK& k) {
+  float om1;
+  const Mom16 m = moments16_les(y, k, om1);
+#pragma unroll
+  for (int q = 0; q < 9; ++q) {
+    float a, b;
+    pair16(q, y[q], y[oppq(q)], m, om1, a, b);
+    s[q] = __float2half_rn(a);
+    s[oppq(q)] = __float2half_rn(b);
+  }
+  s[Q - 1] = __float2half_rn(rest16(y[Q - 1], m, om1));
 }
 
 struct F16 {

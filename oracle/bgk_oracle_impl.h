@@ -359,15 +359,22 @@ static void FN(fast16_cell)(const float *y, float *out, float inv, float om1, co
 }
 
 /* The FP16 form with the Smagorinsky closure (the reference's LES block,
-   SRC/col_MC.F90:221-309, on the FP16 form's moments): with dr, u and a as in
-   fast16_cell and P_q = fmaf(3, cu, fmaf(4.5*cu, cu, a)),
-     t_q = fmaf(dr, P_q, dr + P_q)               (f_eq/w - 1)
-     n_q = y_q*inv - w_q*t_q                      (non-equilibrium, unscaled)
-     Pij from n as in FN(ptotal), pt = Pxx^2 (+ fmaf chain of the others),
-     tau = tauh + 0.5*sqrt(fmaf(cs18, sqrt(pt), tau2)), om = 1/tau,
-     y'_q = fmaf(om*scale*w_q, t_q, (1 - om)*y_q). */
+   SRC/col_MC.F90:221-309, on the FP16 form's moments). With the sums, dr, u
+   and a of fast16_cell and rho = 1 + dr, Pi_neq comes from the second
+   moments of the stored values minus the equilibrium's closed form
+   (D3Q19: sum_q c_a c_b (f_eq - w)_q = dr delta_ab / 3 + rho u_a u_b):
+     Mxx = sp + sm, Myy = jyp + jym, Mzz = jzp + jzm,
+     Mxy = (y2 + y9) - (y0 + y11), Mxz = (y3 + y10) - (y1 + y12),
+     Myz = (y6 + y15) - (y8 + y17),
+     d3 = dr*(1/3), Paa = fmaf(Maa, inv, -fmaf(rho u_a, u_a, d3)),
+     Pab = fmaf(Mab, inv, -(rho u_a * u_b))   (rho u_z formed for Pzz only),
+     pt = Pxx^2 (+ fmaf chain of the others, off-diagonal ones doubled),
+     tau = tauh + 0.5*sqrt(fmaf(cs18, sqrt(pt), tau2)), om = 1/tau;
+   the relaxation is then fast16_cell's pair update with om in place of
+   omega and K = (om*scale)*w per weight class formed per cell. */
 static void FN(fast16_les_cell)(const float *y, float *out, float inv, float scale, float cs18, float tauh,
                                 float tau2) {
+    static const int opp[9] = {11, 12, 9, 10, 13, 14, 15, 16, 17};
     static const int wcls[19] = {2,2,2,2,1,1,2,1,2,2,2,2,2,1,1,2,1,2,0};
     const float wv[3] = {1.0f / 3.0f, 1.0f / 18.0f, 1.0f / 36.0f};
     const float sp = ((y[0] + y[1]) + (y[2] + y[3])) + y[4];
@@ -384,19 +391,15 @@ static void FN(fast16_les_cell)(const float *y, float *out, float inv, float sca
     const float ux = jx * r, uy = (jyp - jym) * r, uz = (jzp - jzm) * r;
     const float usq = fmaf(uz, uz, fmaf(uy, uy, ux * ux));
     const float a = -1.5f * usq;
-    float t[19], nn[19];
-    for (int q = 0; q < 19; ++q) {
-        const float cu = q == 18 ? 0.0f : FN(cdotu16)(q, ux, uy, uz);
-        const float P = fmaf(3.0f, cu, fmaf(4.5f * cu, cu, a));
-        t[q] = fmaf(dr, P, dr + P);
-        nn[q] = y[q] * inv - wv[wcls[q]] * t[q];
-    }
-    const float Pxx = nn[0] + nn[1] + nn[2] + nn[3] + nn[4] + nn[9] + nn[10] + nn[11] + nn[12] + nn[13];
-    const float Pyy = nn[0] + nn[2] + nn[6] + nn[7] + nn[8] + nn[9] + nn[11] + nn[15] + nn[16] + nn[17];
-    const float Pzz = nn[1] + nn[3] + nn[5] + nn[6] + nn[8] + nn[10] + nn[12] + nn[14] + nn[15] + nn[17];
-    const float Pxz = -nn[1] + nn[3] + nn[10] - nn[12];
-    const float Pxy = -nn[0] + nn[2] + nn[9] - nn[11];
-    const float Pyz = nn[6] - nn[8] + nn[15] - nn[17];
+    const float rho = 1.0f + dr;
+    const float d3 = dr * (1.0f / 3.0f);
+    const float rux = rho * ux, ruy = rho * uy;
+    const float Pxx = fmaf(sp + sm, inv, -fmaf(rux, ux, d3));
+    const float Pyy = fmaf(jyp + jym, inv, -fmaf(ruy, uy, d3));
+    const float Pzz = fmaf(jzp + jzm, inv, -fmaf(rho * uz, uz, d3));
+    const float Pxy = fmaf((y[2] + y[9]) - (y[0] + y[11]), inv, -(rux * uy));
+    const float Pxz = fmaf((y[3] + y[10]) - (y[1] + y[12]), inv, -(rux * uz));
+    const float Pyz = fmaf((y[6] + y[15]) - (y[8] + y[17]), inv, -(ruy * uz));
     float pt = Pxx * Pxx;
     pt = fmaf(Pyy, Pyy, pt);
     pt = fmaf(Pzz, Pzz, pt);
@@ -406,7 +409,23 @@ static void FN(fast16_les_cell)(const float *y, float *out, float inv, float sca
     const float tau = tauh + 0.5f * sqrtf(fmaf(cs18, sqrtf(pt), tau2));
     const float om = 1.0f / tau;
     const float om1 = 1.0f - om;
-    for (int q = 0; q < 19; ++q) out[q] = fmaf((om * scale) * wv[wcls[q]], t[q], om1 * y[q]);
+    const float oms = om * scale;
+    float kr3[3], kr45[3], kra[3];
+    for (int c = 0; c < 3; ++c) {
+        const float K = oms * wv[c];
+        const float kd = K * dr, kr = K + kd;
+        kr3[c] = 3.0f * kr;
+        kr45[c] = 4.5f * kr;
+        kra[c] = fmaf(kr, a, kd);
+    }
+    for (int q = 0; q < 9; ++q) {
+        const int c = wcls[q], o = opp[q];
+        const float cu = FN(cdotu16)(q, ux, uy, uz);
+        const float t = fmaf(kr45[c] * cu, cu, kra[c]);
+        out[q] = fmaf(kr3[c], cu, fmaf(om1, y[q], t));
+        out[o] = fmaf(-kr3[c], cu, fmaf(om1, y[o], t));
+    }
+    out[18] = fmaf(om1, y[18], kra[0]);
 }
 #endif
 

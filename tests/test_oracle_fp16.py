@@ -18,7 +18,7 @@ Bound per output value, in scaled units:
     |y16' - scale*f64'| <= ulp16(scale*f64') / 2 + eps * max|y|
 The first term is the binary16 output rounding. The second covers the FP32
 arithmetic of the form (and omega rounded to FP32): eps = 2e-7 for BGK, 1e-6
-for the Smagorinsky closure (measured worst cases 4.5e-8 and 2.5e-7 of
+for the Smagorinsky closure (measured worst cases 4.5e-8 and 2.0e-7 of
 max|y| over these sets).
 """
 import numpy as np

@@ -11,8 +11,6 @@
 //                per-block partials
 //   k_enstrophy  0.5|curl u|^2 from the local velocity field
 //   k_shift3     shift-only stencil of SRC/do_somethingGPU.F90:37-100
-#include <cstdlib>
-
 #include "kernels.h"
 #include "reduce.cuh"
 
@@ -163,25 +161,30 @@ struct XLanes {
   }
 };
 
-// Elements i0 + cx ... i0 + 3 + cx of a row whose aligned four elements
-// at i0 are A (pull of the four cells i0..i0+3 along c with cx = -c_x of the
-// pull); `p` is the row, i_prev / i_next its periodic neighbours of the chunk.
-__device__ __forceinline__ uint2 shift_in(uint2 A, int cx, const __half* p, int i_prev, int i_next,
-                                          const XLanes& xl) {
-  if (cx == 0) return A;
-  uint2 Y;
-  if (cx > 0) {  // elements i0-1 .. i0+2
-    unsigned prev = __shfl_sync(0xffffffffu, A.y >> 16, xl.src_prev);
-    if (xl.edge_prev) prev = ldg_u16(p + i_prev);
-    Y.x = __byte_perm(A.x, prev, 0x1054);
-    Y.y = __byte_perm(A.x, A.y, 0x5432);
-  } else {  // elements i0+1 .. i0+4
-    unsigned next = __shfl_sync(0xffffffffu, A.x & 0xffffu, xl.src_next);
-    if (xl.edge_next) next = ldg_u16(p + i_next);
-    Y.x = __byte_perm(A.x, A.y, 0x5432);
-    Y.y = __byte_perm(A.y, next, 0x5432);
+// Second half of the x-shifted row loads of the four-cells-per-thread FP16
+// kernels. Y[q] holds the aligned chunk of elements i0..i0+3 of population
+// q's source row; cells i0..i0+3 need elements i0 - cx ... i0 + 3 - cx with
+// cx = c_q,x, so the element that crosses the chunk boundary comes from the
+// neighbouring lane (warp shuffle) or, for a warp's edge lane, from E[q],
+// which that lane loaded together with the chunks. All loads are issued
+// before the first shuffle: measured on B200 (FP16 AA odd step, 256^3), this
+// ordering lifted the pair of AA steps from 72.2 to 75.6 GLUPS.
+__device__ __forceinline__ void shift_rows(uint2 (&Y)[Q], const unsigned short (&E)[Q], const XLanes& xl) {
+#pragma unroll
+  for (int q = 0; q < Q; ++q) {
+    const uint2 A = Y[q];
+    if (cxq(q) > 0) {  // elements i0-1 .. i0+2
+      unsigned prev = __shfl_sync(0xffffffffu, A.y >> 16, xl.src_prev);
+      if (xl.edge_prev) prev = E[q];
+      Y[q].x = __byte_perm(A.x, prev, 0x1054);
+      Y[q].y = __byte_perm(A.x, A.y, 0x5432);
+    } else if (cxq(q) < 0) {  // elements i0+1 .. i0+4
+      unsigned next = __shfl_sync(0xffffffffu, A.x & 0xffffu, xl.src_next);
+      if (xl.edge_next) next = E[q];
+      Y[q].x = __byte_perm(A.x, A.y, 0x5432);
+      Y[q].y = __byte_perm(A.y, next, 0x5432);
+    }
   }
-  return Y;
 }
 
 // Stores four cells' values Y (cells i0..i0+3) at elements i0 + cx ...
@@ -224,44 +227,25 @@ __global__ void __launch_bounds__(128, 6) k_two_f16v(Pops<const __half> src, Pop
   const int j = t >> log_tpr, pos = t & (tpr - 1);
   const int k = blockIdx.y + k0;  // planes k0 .. k0 + gridDim.y - 1
   if (j >= g.ny) return;  // whole warps: ny*tpr is a multiple of 32
-  const int lane = threadIdx.x & 31;
+  const XLanes xl(tpr, pos, threadIdx.x & 31);
   const int i0 = pos * 4;
   const int jm = j == 0 ? g.ny - 1 : j - 1, jp = j == g.ny - 1 ? 0 : j + 1;
   const int km = k == 0 ? g.nz - 1 : k - 1, kp = k == g.nz - 1 ? 0 : k + 1;
-  int src_prev, src_next;
-  bool load_prev = false, load_next = false;
-  if (tpr >= 32) {
-    src_prev = (lane + 31) & 31;
-    src_next = (lane + 1) & 31;
-    load_prev = lane == 0;
-    load_next = lane == 31;
-  } else {
-    src_prev = pos == 0 ? lane + tpr - 1 : lane - 1;
-    src_next = pos == tpr - 1 ? lane - tpr + 1 : lane + 1;
-  }
   const int i_prev = pos == 0 ? g.nx - 1 : i0 - 1;
   const int i_next = pos == tpr - 1 ? 0 : i0 + 4;
   uint2 Y[Q];  // four cells' stored values per population, cell m in half m
+  unsigned short E[Q];
 #pragma unroll
   for (int q = 0; q < Q; ++q) {
     const int jj = cyq(q) > 0 ? jm : (cyq(q) < 0 ? jp : j);
     const int kk = czq(q) > 0 ? km : (czq(q) < 0 ? kp : k);
     const __half* p = (q == Q - 1 ? (const __half*)dst.p[Q - 1] : src.p[q]) + g.sx * (jj + g.ny * kk);
-    const uint2 A = (q == Q - 1) ? *reinterpret_cast<const uint2*>(p + i0) : __ldg(reinterpret_cast<const uint2*>(p + i0));
-    if (cxq(q) == 0) {
-      Y[q] = A;
-    } else if (cxq(q) > 0) {  // cells need elements i0-1 .. i0+2
-      unsigned prev = __shfl_sync(0xffffffffu, A.y >> 16, src_prev);
-      if (load_prev) prev = ldg_u16(p + i_prev);
-      Y[q].x = __byte_perm(A.x, prev, 0x1054);
-      Y[q].y = __byte_perm(A.x, A.y, 0x5432);
-    } else {  // cells need elements i0+1 .. i0+4
-      unsigned next = __shfl_sync(0xffffffffu, A.x & 0xffffu, src_next);
-      if (load_next) next = ldg_u16(p + i_next);
-      Y[q].x = __byte_perm(A.x, A.y, 0x5432);
-      Y[q].y = __byte_perm(A.y, next, 0x5432);
-    }
+    Y[q] = (q == Q - 1) ? *reinterpret_cast<const uint2*>(p + i0) : __ldg(reinterpret_cast<const uint2*>(p + i0));
+    E[q] = 0;
+    if (cxq(q) > 0 && xl.edge_prev) E[q] = ldg_u16(p + i_prev);
+    if (cxq(q) < 0 && xl.edge_next) E[q] = ldg_u16(p + i_next);
   }
+  shift_rows(Y, E, xl);
   collide4_f16<LES>(Y, K);
   const int o = i0 + g.sx * (j + g.ny * k);
 #pragma unroll
@@ -407,43 +391,13 @@ __global__ void __launch_bounds__(256, 5) k_aa_f16_odd(Pops<__half> a, Geo g, St
 // 62.8-65.0 with two cells per thread on the odd step, and 58 for one cell per
 // thread. The LES odd step recomputes its store rows the same way (96 registers,
 // a few spilled bytes, 5 blocks per SM).
-__device__ __forceinline__ void prefetch_l2(const void* p, unsigned bytes) {
-  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
-}
-
-// Rows of the block `ahead` blocks after this one (grid order): lanes 0..18
-// of each warp ask the L2 for one population's 256-byte segment of that
-// warp's rows (tpr >= 32 only, so a warp covers one row segment).
-template <bool ODD>
-__device__ __forceinline__ void prefetch_rows_ahead(const Pops<__half>& a, const Geo& g, int log_tpr, int ahead) {
-  const int lane = threadIdx.x & 31;
-  if (ahead <= 0 || log_tpr < 5 || lane >= Q) return;
-  const long long nb = (long long)gridDim.x * gridDim.y;
-  const long long b = blockIdx.x + (long long)gridDim.x * blockIdx.y + ahead;
-  if (b >= nb) return;
-  const int bx = (int)(b % gridDim.x), k = (int)(b / gridDim.x);
-  const int t = bx * blockDim.x + (threadIdx.x & ~31);
-  const int j = t >> log_tpr, i0 = (t & ((1 << log_tpr) - 1)) * 4;
-  if (j >= g.ny) return;
-  const int q = lane;
-  int jj = j, kk = k;
-  if (ODD) {
-    jj = wrapi(j - cyq(q), g.ny);
-    kk = wrapi(k - czq(q), g.nz);
-  }
-  const __half* p = a.p[ODD ? oppq(q) : q] + g.sx * (jj + g.ny * kk) + i0;
-  prefetch_l2(p, 256);
-}
-
-template <bool ODD, bool LES, int VAR = 0>
-__global__ void __launch_bounds__(128, ODD ? 5 : 6) k_aa_f16v(Pops<__half> a, Geo g, StepK K,
-                                                                          int log_tpr, int ahead = 0) {
+template <bool ODD, bool LES>
+__global__ void __launch_bounds__(128, ODD ? 5 : 6) k_aa_f16v(Pops<__half> a, Geo g, StepK K, int log_tpr) {
   const int tpr = 1 << log_tpr;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = t >> log_tpr, pos = t & (tpr - 1);
   const int k = blockIdx.y;
   if (j >= g.ny) return;  // whole warps: ny*tpr is a multiple of 32
-  if (VAR & 2) prefetch_rows_ahead<ODD>(a, g, log_tpr, ahead);
   const XLanes xl(tpr, pos, threadIdx.x & 31);
   const int i0 = pos * 4;
   const int jm = j == 0 ? g.ny - 1 : j - 1, jp = j == g.ny - 1 ? 0 : j + 1;
@@ -456,8 +410,7 @@ __global__ void __launch_bounds__(128, ODD ? 5 : 6) k_aa_f16v(Pops<__half> a, Ge
     return g.sx * (jj + g.ny * kk);
   };
   uint2 Y[Q];
-  if (ODD && (VAR & 1)) {
-    // every row load and crossing-element load issued before any shuffle
+  if (ODD) {
     unsigned short E[Q];
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
@@ -467,31 +420,10 @@ __global__ void __launch_bounds__(128, ODD ? 5 : 6) k_aa_f16v(Pops<__half> a, Ge
       if (cxq(q) > 0 && xl.edge_prev) E[q] = ldg_u16(p + i_prev);
       if (cxq(q) < 0 && xl.edge_next) E[q] = ldg_u16(p + i_next);
     }
-#pragma unroll
-    for (int q = 0; q < Q; ++q) {
-      const uint2 A = Y[q];
-      if (cxq(q) > 0) {
-        unsigned prev = __shfl_sync(0xffffffffu, A.y >> 16, xl.src_prev);
-        if (xl.edge_prev) prev = E[q];
-        Y[q].x = __byte_perm(A.x, prev, 0x1054);
-        Y[q].y = __byte_perm(A.x, A.y, 0x5432);
-      } else if (cxq(q) < 0) {
-        unsigned next = __shfl_sync(0xffffffffu, A.x & 0xffffu, xl.src_next);
-        if (xl.edge_next) next = E[q];
-        Y[q].x = __byte_perm(A.x, A.y, 0x5432);
-        Y[q].y = __byte_perm(A.y, next, 0x5432);
-      }
-    }
+    shift_rows(Y, E, xl);
   } else {
 #pragma unroll
-    for (int q = 0; q < Q; ++q) {
-      if (!ODD) {
-        Y[q] = __ldg(reinterpret_cast<const uint2*>(a.p[q] + row(0, 0) + i0));
-      } else {
-        const __half* p = a.p[oppq(q)] + row(-cyq(q), -czq(q));
-        Y[q] = shift_in(__ldg(reinterpret_cast<const uint2*>(p + i0)), cxq(q), p, i_prev, i_next, xl);
-      }
-    }
+    for (int q = 0; q < Q; ++q) Y[q] = __ldg(reinterpret_cast<const uint2*>(a.p[q] + row(0, 0) + i0));
   }
   collide4_f16<LES>(Y, K);
   int js = j, ks = k;  // store rows: recomputed after the collision (BGK odd step)
@@ -1092,34 +1024,8 @@ static cudaError_t aa_impl(const Lattice& a, int odd, const StepK& K, int varian
   // FP16: four cells per thread where the box fits it (automatic or 4)
   if (lt4 >= 0) {
     const dim3 grid = f16v_grid(a.g, lt4, a.g.nz);
-    static int var = -1, mult = 1;
-    if (var < 0) {
-      const char* e = getenv("BGK_AA_VARIANT");
-      var = e ? atoi(e) : 0;
-      const char* m = getenv("BGK_AA_AHEAD");
-      mult = m ? atoi(m) : 1;
-    }
-    int ahead = 0;
-    if (var & 6) {
-      int dev = 0, nsm = 148, bps = 1;
-      cudaGetDevice(&dev);
-      cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-      if (odd) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_aa_f16v<true, false, 3>, 128, 0);
-      else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_aa_f16v<false, false, 2>, 128, 0);
-      ahead = nsm * bps * mult;
-    }
-    auto P = pops_of<__half>(a);
-    if (odd) {
-      switch (var & 3) {
-        case 0: k_aa_f16v<true, false, 0><<<grid, 128, 0, st>>>(P, a.g, K, lt4, 0); break;
-        case 1: k_aa_f16v<true, false, 1><<<grid, 128, 0, st>>>(P, a.g, K, lt4, 0); break;
-        case 2: k_aa_f16v<true, false, 2><<<grid, 128, 0, st>>>(P, a.g, K, lt4, ahead); break;
-        case 3: k_aa_f16v<true, false, 3><<<grid, 128, 0, st>>>(P, a.g, K, lt4, ahead); break;
-      }
-    } else {
-      if (var & 4) k_aa_f16v<false, false, 2><<<grid, 128, 0, st>>>(P, a.g, K, lt4, ahead);
-      else k_aa_f16v<false, false, 0><<<grid, 128, 0, st>>>(P, a.g, K, lt4, 0);
-    }
+    if (odd) k_aa_f16v<true, false><<<grid, 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
+    else k_aa_f16v<false, false><<<grid, 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
     return cudaGetLastError();
   }
   if (odd && F::id == FORM_F16)

@@ -57,7 +57,7 @@ def test_tiled_box_evolves_as_its_tile(bgk, tmp_path, L, form, scheme):
             want = ds[f] * (rep ** 3 if f == "diss" else 1)  # diss is a sum over the cells, the others means
             assert db[f] == pytest.approx(want, rel=1e-12, abs=1e-15), f
         for kind in ("xy", "xz", "yz"):
-            for idx in (1, 2, n, n + 1, 2 * n + 37, L):
+            for idx in (1, 2, n, n + 1, n + 37, L - 5, L):
                 got = _slice(big, kind, idx, steps, tmp_path).reshape(L, L, 3)
                 ref = _slice(small, kind, (idx - 1) % n + 1, steps, tmp_path).reshape(n, n, 3)
                 assert np.array_equal(got, np.tile(ref, (rep, rep, 1))), (kind, idx)

@@ -11,8 +11,6 @@
 //                per-block partials
 //   k_enstrophy  0.5|curl u|^2 from the local velocity field
 //   k_shift3     shift-only stencil of SRC/do_somethingGPU.F90:37-100
-#include <cstdlib>
-
 #include "kernels.h"
 #include "reduce.cuh"
 
@@ -142,32 +140,6 @@ __device__ __forceinline__ void collide4_f16(uint2 (&Y)[Q], const StepK& K) {
   }
 }
 
-template <bool LES>
-__device__ __forceinline__ void collide4_f16x2(uint2 (&Y)[Q], const StepK& K) {
-#pragma unroll
-  for (int h = 0; h < 2; ++h) {
-    float2 om1 = f2(K.om1);
-    Mom16x2 M;
-    {
-      float2 y[Q];  // cells (2h, 2h + 1), lane by lane
-#pragma unroll
-      for (int q = 0; q < Q; ++q) y[q] = u2f2(h ? Y[q].y : Y[q].x);
-      if constexpr (LES) M = moments16x2_les(y, K, om1);
-      else M = moments16x2(y, K);
-    }
-#pragma unroll
-    for (int q = 0; q < 9; ++q) {
-      const int r = oppq(q);
-      float2 p, o;
-      pair16x2(q, u2f2(h ? Y[q].y : Y[q].x), u2f2(h ? Y[r].y : Y[r].x), M, om1, p, o);
-      const unsigned pq = h2u(__float22half2_rn(p)), pr = h2u(__float22half2_rn(o));
-      if (h) { Y[q].y = pq; Y[r].y = pr; } else { Y[q].x = pq; Y[r].x = pr; }
-    }
-    const unsigned pz = h2u(__float22half2_rn(rest16x2(u2f2(h ? Y[Q - 1].y : Y[Q - 1].x), M, om1)));
-    if (h) Y[Q - 1].y = pz; else Y[Q - 1].x = pz;
-  }
-}
-
 // Lanes that exchange x-neighbours in the four-cells-per-thread FP16 kernels:
 // a row of nx cells is tpr = nx/4 consecutive threads. Rows shorter than a warp
 // wrap inside it; rows of one or more warps wrap through global memory at the
@@ -247,7 +219,7 @@ __device__ __forceinline__ void shift_out(uint2 Y, int cx, __half* p, int i0, in
   }
 }
 
-template <bool LES, bool PK = false>
+template <bool LES>
 __global__ void __launch_bounds__(128, 6) k_two_f16v(Pops<const __half> src, Pops<__half> dst, Geo g, StepK K,
                                                   int log_tpr, int k0) {
   const int tpr = 1 << log_tpr;
@@ -274,8 +246,7 @@ __global__ void __launch_bounds__(128, 6) k_two_f16v(Pops<const __half> src, Pop
     if (cxq(q) < 0 && xl.edge_next) E[q] = ldg_u16(p + i_next);
   }
   shift_rows(Y, E, xl);
-  if constexpr (PK) collide4_f16x2<LES>(Y, K);
-  else collide4_f16<LES>(Y, K);
+  collide4_f16<LES>(Y, K);
   const int o = i0 + g.sx * (j + g.ny * k);
 #pragma unroll
   for (int q = 0; q < Q; ++q) *reinterpret_cast<uint2*>(dst.p[q] + o) = Y[q];
@@ -420,7 +391,7 @@ __global__ void __launch_bounds__(256, 5) k_aa_f16_odd(Pops<__half> a, Geo g, St
 // 62.8-65.0 with two cells per thread on the odd step, and 58 for one cell per
 // thread. The LES odd step recomputes its store rows the same way (96 registers,
 // a few spilled bytes, 5 blocks per SM).
-template <bool ODD, bool LES, bool PK = false>
+template <bool ODD, bool LES>
 __global__ void __launch_bounds__(128, ODD ? 5 : 6) k_aa_f16v(Pops<__half> a, Geo g, StepK K, int log_tpr) {
   const int tpr = 1 << log_tpr;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -454,8 +425,7 @@ __global__ void __launch_bounds__(128, ODD ? 5 : 6) k_aa_f16v(Pops<__half> a, Ge
 #pragma unroll
     for (int q = 0; q < Q; ++q) Y[q] = __ldg(reinterpret_cast<const uint2*>(a.p[q] + row(0, 0) + i0));
   }
-  if constexpr (PK) collide4_f16x2<LES>(Y, K);
-  else collide4_f16<LES>(Y, K);
+  collide4_f16<LES>(Y, K);
   int js = j, ks = k;  // store rows: recomputed after the collision (BGK odd step)
   if (ODD) asm volatile("" : "+r"(js), "+r"(ks));
   const int jms = js == 0 ? g.ny - 1 : js - 1, jps = js == g.ny - 1 ? 0 : js + 1;
@@ -949,15 +919,6 @@ static dim3 f16v_grid(const Geo& g, int log_tpr, int planes) {
 }
 
 // log2(nx/V) when the V-cells-per-thread FP16 kernel applies, else -1.
-static bool f16_packed() {
-  static int v = -1;
-  if (v < 0) {
-    const char* e = getenv("BGK_F16_PACKED");
-    v = e ? atoi(e) : 0;
-  }
-  return v != 0;
-}
-
 static int f16v_log_tpr(const Geo& g, int V) {
   if (g.nx % V) return -1;
   const int tpr = g.nx / V;
@@ -981,7 +942,7 @@ static cudaError_t two_impl(const Lattice& s, const Lattice& d, const StepK& K, 
       Pops<__half> ph = pops_of<__half>(d);
       ph.p[Q - 1] = (__half*)s.p[Q - 1];
       const dim3 grid = f16v_grid(s.g, lt, s.g.nz);
-      { if (f16_packed()) k_two_f16v<true, true><<<grid, 128, 0, st>>>(pops_of<const __half>(s), ph, s.g, K, lt, 0); else k_two_f16v<true><<<grid, 128, 0, st>>>(pops_of<const __half>(s), ph, s.g, K, lt, 0); }
+      k_two_f16v<true><<<grid, 128, 0, st>>>(pops_of<const __half>(s), ph, s.g, K, lt, 0);
     } else {
       k_two<F, true><<<sh.grid, sh.block, 0, st>>>(ps, pd, s.g, K);
     }
@@ -1004,8 +965,7 @@ static cudaError_t two_impl(const Lattice& s, const Lattice& d, const StepK& K, 
       dim3 grid((unsigned)((threads + (V == 4 ? 127 : 255)) / (V == 4 ? 128 : 256)), s.g.nz);
       Pops<__half> ph = pops_of<__half>(d);
       ph.p[Q - 1] = (__half*)s.p[Q - 1];
-      if (V == 4 && f16_packed()) k_two_f16v<false, true><<<grid, 128, 0, st>>>(pops_of<const __half>(s), ph, s.g, K, lt, 0);
-      else if (V == 4) k_two_f16v<false><<<grid, 128, 0, st>>>(pops_of<const __half>(s), ph, s.g, K, lt, 0);
+      if (V == 4) k_two_f16v<false><<<grid, 128, 0, st>>>(pops_of<const __half>(s), ph, s.g, K, lt, 0);
       else k_two_f16v2<<<grid, 256, 0, st>>>(pops_of<const __half>(s), ph, s.g, K, lt);
       return cudaGetLastError();
     }
@@ -1047,8 +1007,7 @@ static cudaError_t aa_impl(const Lattice& a, int odd, const StepK& K, int varian
   if (K.les) {
     if (lt4 >= 0) {
       const dim3 grid = f16v_grid(a.g, lt4, a.g.nz);
-      if (f16_packed()) { if (odd) k_aa_f16v<true, true, true><<<grid, 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt4); else k_aa_f16v<false, true, true><<<grid, 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt4); }
-      else if (odd) k_aa_f16v<true, true><<<grid, 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
+      if (odd) k_aa_f16v<true, true><<<grid, 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
       else k_aa_f16v<false, true><<<grid, 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
     } else if (odd) {
       k_aa<F, true, true><<<sh.grid, sh.block, 0, st>>>(pops_of<S>(a), a.g, K);
@@ -1065,8 +1024,7 @@ static cudaError_t aa_impl(const Lattice& a, int odd, const StepK& K, int varian
   // FP16: four cells per thread where the box fits it (automatic or 4)
   if (lt4 >= 0) {
     const dim3 grid = f16v_grid(a.g, lt4, a.g.nz);
-    if (f16_packed()) { if (odd) k_aa_f16v<true, false, true><<<grid, 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt4); else k_aa_f16v<false, false, true><<<grid, 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt4); }
-    else if (odd) k_aa_f16v<true, false><<<grid, 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
+    if (odd) k_aa_f16v<true, false><<<grid, 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
     else k_aa_f16v<false, false><<<grid, 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
     return cudaGetLastError();
   }

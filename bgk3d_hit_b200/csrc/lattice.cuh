@@ -287,125 +287,6 @@ __device__ __forceinline__ void cell16_les(const float (&y)[Q], __half (&s)[Q], 
   s[Q - 1] = __float2half_rn(rest16(y[Q - 1], m, om1));
 }
 
-// The same collision on two cells at once, lane by lane in packed FP32
-// (sm_100's paired add / multiply / fused multiply-add, each lane rounded to
-// nearest like the scalar operation): every lane performs exactly the
-// operations of moments16 / pair16 / rest16 / moments16_les, so the two
-// cells' results are the scalar form's bits with about half the FP32
-// instructions. Reciprocal, division and square roots stay scalar per lane.
-struct Mom16x2 { float2 dr, ux, uy, uz, a, kr3[3], kr45[3], kra[3]; };
-
-__device__ __forceinline__ float2 f2(float v) { return make_float2(v, v); }
-__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
-__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
-__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
-__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
-__device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
-
-// The sums of moments16 on two cells.
-struct Sums16x2 { float2 sp, sm, sum, jx, jyp, jym, jzp, jzm; };
-__device__ __forceinline__ Sums16x2 sums16x2(const float2 (&y)[Q]) {
-  Sums16x2 t;
-  t.sp = add2(add2(add2(y[0], y[1]), add2(y[2], y[3])), y[4]);
-  t.sm = add2(add2(add2(y[9], y[10]), add2(y[11], y[12])), y[13]);
-  const float2 s0 = add2(add2(add2(add2(y[5], y[6]), add2(y[7], y[8])), add2(add2(y[14], y[15]), add2(y[16], y[17]))),
-                         y[18]);
-  t.sum = add2(add2(t.sp, t.sm), s0);
-  t.jx = sub2(t.sp, t.sm);
-  t.jyp = add2(add2(add2(y[2], y[6]), add2(y[7], y[8])), y[11]);
-  t.jym = add2(add2(add2(y[0], y[9]), add2(y[15], y[16])), y[17]);
-  t.jzp = add2(add2(add2(y[3], y[5]), add2(y[6], y[12])), y[17]);
-  t.jzm = add2(add2(add2(y[1], y[8]), add2(y[10], y[14])), y[15]);
-  return t;
-}
-
-// dr, u, a of moments16 on two cells; rp = 1 + dr.
-__device__ __forceinline__ void vel16x2(const Sums16x2& t, const StepK& k, Mom16x2& m, float2& rp) {
-  m.dr = mul2(t.sum, f2(k.inv));
-  rp = add2(f2(1.0f), m.dr);
-  const float2 r = mul2(f2(k.inv), make_float2(__frcp_rn(rp.x), __frcp_rn(rp.y)));
-  m.ux = mul2(t.jx, r);
-  m.uy = mul2(sub2(t.jyp, t.jym), r);
-  m.uz = mul2(sub2(t.jzp, t.jzm), r);
-  const float2 usq = fma2(m.uz, m.uz, fma2(m.uy, m.uy, mul2(m.ux, m.ux)));
-  m.a = mul2(f2(-1.5f), usq);
-}
-
-// kr3, kr45, kra of one weight class from K (per lane) and dr.
-__device__ __forceinline__ void krs16x2(Mom16x2& m, int c, float2 K) {
-  const float2 kd = mul2(K, m.dr);
-  const float2 kr = add2(K, kd);
-  m.kr3[c] = mul2(f2(3.0f), kr);
-  m.kr45[c] = mul2(f2(4.5f), kr);
-  m.kra[c] = fma2(kr, m.a, kd);
-}
-
-__device__ __forceinline__ Mom16x2 moments16x2(const float2 (&y)[Q], const StepK& k) {
-  const Sums16x2 t = sums16x2(y);
-  Mom16x2 m;
-  float2 rp;
-  vel16x2(t, k, m, rp);
-#pragma unroll
-  for (int c = 0; c < 3; ++c) krs16x2(m, c, f2(k.kw[c]));
-  return m;
-}
-
-// moments16_les on two cells: om1 receives 1 - omega_eff per lane.
-__device__ __forceinline__ Mom16x2 moments16x2_les(const float2 (&y)[Q], const StepK& k, float2& om1) {
-  const Sums16x2 t = sums16x2(y);
-  Mom16x2 m;
-  float2 rp;
-  vel16x2(t, k, m, rp);
-  const float2 inv = f2(k.inv);
-  const float2 d3 = mul2(m.dr, f2(1.0f / 3.0f));
-  const float2 rux = mul2(rp, m.ux), ruy = mul2(rp, m.uy);
-  const float2 Pxx = fma2(add2(t.sp, t.sm), inv, neg2(fma2(rux, m.ux, d3)));
-  const float2 Pyy = fma2(add2(t.jyp, t.jym), inv, neg2(fma2(ruy, m.uy, d3)));
-  const float2 Pzz = fma2(add2(t.jzp, t.jzm), inv, neg2(fma2(mul2(rp, m.uz), m.uz, d3)));
-  const float2 Pxy = fma2(sub2(add2(y[2], y[9]), add2(y[0], y[11])), inv, neg2(mul2(rux, m.uy)));
-  const float2 Pxz = fma2(sub2(add2(y[3], y[10]), add2(y[1], y[12])), inv, neg2(mul2(rux, m.uz)));
-  const float2 Pyz = fma2(sub2(add2(y[6], y[15]), add2(y[8], y[17])), inv, neg2(mul2(ruy, m.uz)));
-  float2 pt = mul2(Pxx, Pxx);
-  pt = fma2(Pyy, Pyy, pt);
-  pt = fma2(Pzz, Pzz, pt);
-  pt = fma2(mul2(f2(2.0f), Pxy), Pxy, pt);
-  pt = fma2(mul2(f2(2.0f), Pxz), Pxz, pt);
-  pt = fma2(mul2(f2(2.0f), Pyz), Pyz, pt);
-  const float2 sq = make_float2(__fsqrt_rn(__fmaf_rn(k.cs18_f, __fsqrt_rn(pt.x), k.tau2_f)),
-                                __fsqrt_rn(__fmaf_rn(k.cs18_f, __fsqrt_rn(pt.y), k.tau2_f)));
-  const float2 tau = add2(f2(k.tauh_f), mul2(f2(0.5f), sq));
-  const float2 om = make_float2(__fdiv_rn(1.0f, tau.x), __fdiv_rn(1.0f, tau.y));
-  om1 = sub2(f2(1.0f), om);
-  const float2 oms = mul2(om, f2(k.scale));
-#pragma unroll
-  for (int c = 0; c < 3; ++c) krs16x2(m, c, mul2(oms, f2(c == 0 ? 1.0f / 3.0f : (c == 1 ? 1.0f / 18.0f : 1.0f / 36.0f))));
-  return m;
-}
-
-// c_q.u of pair16 (first non-zero component, plus the second one if any).
-__device__ __forceinline__ float2 cdotu2(int q, const Mom16x2& m) {
-  const int cx = cxq(q), cy = cyq(q), cz = czq(q);
-  float2 cu = f2(0.0f);
-  bool first = true;
-  if (cx != 0) { cu = cx > 0 ? m.ux : neg2(m.ux); first = false; }
-  if (cy != 0) { const float2 t = cy > 0 ? m.uy : neg2(m.uy); cu = first ? t : add2(cu, t); first = false; }
-  if (cz != 0) { const float2 t = cz > 0 ? m.uz : neg2(m.uz); cu = first ? t : add2(cu, t); }
-  return cu;
-}
-
-__device__ __forceinline__ void pair16x2(int q, float2 yq, float2 yo, const Mom16x2& m, float2 om1, float2& oq,
-                                         float2& oo) {
-  const int c = wclass(q);
-  const float2 cu = cdotu2(q, m);
-  const float2 t = fma2(mul2(m.kr45[c], cu), cu, m.kra[c]);
-  oq = fma2(m.kr3[c], cu, fma2(om1, yq, t));
-  oo = fma2(neg2(m.kr3[c]), cu, fma2(om1, yo, t));
-}
-
-__device__ __forceinline__ float2 rest16x2(float2 y, const Mom16x2& m, float2 om1) {
-  return fma2(om1, y, m.kra[0]);
-}
-
 struct F16 {
   using S = __half; using R = float; using V = Ex<float>;
   static constexpr int id = 2;

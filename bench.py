@@ -186,11 +186,13 @@ def kernel_key(precision, scheme, L, kernel=0, les=False):
     """Name of the stream-collide kernel a launch runs (the key of
     profiles/ncu_traffic.json)."""
     kern = f"{'k_two' if scheme == 'two_lattice' else 'k_aa'}_{precision}" + ("_les" if les else "")
-    if precision == "fp16" and not les and kernel in ((0, 2, 4) if scheme == "two_lattice" else (0, 4)):
+    allowed = (0, 4) if (les or scheme == "aa") else (0, 2, 4)  # the LES collision runs on four cells only
+    if precision == "fp16" and kernel in allowed:
         v = 2 if kernel == 2 else 4
         tpr = L // v
         if L % v == 0 and tpr & (tpr - 1) == 0 and (L * tpr) % 32 == 0:  # cells per thread: 2 or 4
             kern = ("k_two_f16v2" if kernel == 2 else "k_two_f16v") if scheme == "two_lattice" else "k_aa_f16v"
+            kern += "_les" if les else ""
     return kern
 
 

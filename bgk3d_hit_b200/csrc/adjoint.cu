@@ -99,8 +99,10 @@ __global__ void __launch_bounds__(DIAG_THREADS) k_adj_terminal(Pops<const typena
 // pulled from x - c_q and lam gathered from x + c_q (lam_q(x) = mu_q(x + c_q)
 // of the previous adjoint step), both as row loads like the forward kernel's;
 // lam is read again from cache for the output, mu_q(x), stored at the cell.
-// rho and u are formed in the form's arithmetic R, the moment sums and A, B,
-// G in double. Each block adds its dL/domega
+// rho, u, the moment sums and A, B, G are formed in the form's arithmetic
+// (double for FP64, float for FP32: in double the FP32 step was bound by the
+// FP64 pipe rather than by its half-size loads); each cell's dL/domega term is
+// added to the block's sum in double. Each block adds its dL/domega
 // contribution (warp shuffles, then the four warp sums in order) into its
 // own compensated pair acc[2*block].
 template <class F>
@@ -108,6 +110,7 @@ __global__ void __launch_bounds__(128, 4) k_adj_step(Pops<const typename F::S> f
                                                      Pops<typename F::S> lout, Geo g, typename F::R omega,
                                                      double* acc) {
   using S = typename F::S; using R = typename F::R;
+  using D = R;  // arithmetic of the moment sums: the form's (double for FP64, float for FP32)
   __shared__ double wsum[4];
   double dw = 0.0;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -127,17 +130,17 @@ __global__ void __launch_bounds__(128, 4) k_adj_step(Pops<const typename F::S> f
       return ii + g.sx * (jj + g.ny * kk);
     };
     R rho = (R)1, jx = 0, jy = 0, jz = 0;
-    double L0 = 0, m1x = 0, m1y = 0, m1z = 0, mxx = 0, myy = 0, mzz = 0, mxy = 0, mxz = 0, myz = 0, S1 = 0;
+    D L0 = 0, m1x = 0, m1y = 0, m1z = 0, mxx = 0, myy = 0, mzz = 0, mxy = 0, mxz = 0, myz = 0, S1 = 0;
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
       const R x = (R)__ldg(ft.p[q] + offq(q, 1));
-      const double lam = (double)__ldg(lin.p[q] + offq(q, -1));
+      const D lam = (D)__ldg(lin.p[q] + offq(q, -1));
       rho += x;
       jx += (R)cxq(q) * x;
       jy += (R)cyq(q) * x;
       jz += (R)czq(q) * x;
-      S1 += lam * (double)x;
-      const double wl = wq<double>(q) * lam;
+      S1 += lam * (D)x;
+      const D wl = wq<D>(q) * lam;
       L0 += wl;
       m1x += cxq(q) * wl;
       m1y += cyq(q) * wl;
@@ -150,23 +153,23 @@ __global__ void __launch_bounds__(128, 4) k_adj_step(Pops<const typename F::S> f
       myz += (cyq(q) * czq(q)) * wl;
     }
     const R ri = (R)1 / rho;
-    const double ux = (double)(jx * ri), uy = (double)(jy * ri), uz = (double)(jz * ri);
-    const double a = -1.5 * (ux * ux + uy * uy + uz * uz);
-    const double nx = mxx * ux + mxy * uy + mxz * uz;  // M2 u
-    const double ny = mxy * ux + myy * uy + myz * uz;
-    const double nz = mxz * ux + myz * uy + mzz * uz;
-    const double A = L0 * (1.0 + a) + 3.0 * (ux * m1x + uy * m1y + uz * m1z) + 4.5 * (ux * nx + uy * ny + uz * nz);
-    const double Bx = 3.0 * (m1x + 3.0 * nx - ux * L0);
-    const double By = 3.0 * (m1y + 3.0 * ny - uy * L0);
-    const double Bz = 3.0 * (m1z + 3.0 * nz - uz * L0);
-    const double G = A - (Bx * ux + By * uy + Bz * uz);
-    dw = (double)rho * A - L0 - S1;
+    const D ux = (D)(jx * ri), uy = (D)(jy * ri), uz = (D)(jz * ri);
+    const D a = (D)-1.5 * (ux * ux + uy * uy + uz * uz);
+    const D nx = mxx * ux + mxy * uy + mxz * uz;  // M2 u
+    const D ny = mxy * ux + myy * uy + myz * uz;
+    const D nz = mxz * ux + myz * uy + mzz * uz;
+    const D A = L0 * ((D)1 + a) + (D)3 * (ux * m1x + uy * m1y + uz * m1z) + (D)4.5 * (ux * nx + uy * ny + uz * nz);
+    const D Bx = (D)3 * (m1x + (D)3 * nx - ux * L0);
+    const D By = (D)3 * (m1y + (D)3 * ny - uy * L0);
+    const D Bz = (D)3 * (m1z + (D)3 * nz - uz * L0);
+    const D G = A - (Bx * ux + By * uy + Bz * uz);
+    dw = (double)((D)rho * A - L0 - S1);
     const R om1 = (R)1 - omega;
     const R om = omega;
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
       const R lam = (R)__ldg(lin.p[q] + offq(q, -1));
-      const R gq = (R)(G + cdot<double>(q, Bx, By, Bz));
+      const R gq = (R)(G + cdot<D>(q, Bx, By, Bz));
       const R mu = om1 * lam + om * gq;
       lout.p[q][o] = (S)mu;  // mu_q(x): cell x - c_q of the next adjoint step gathers it as its lam_q
     }

@@ -11,8 +11,6 @@
 //                per-block partials
 //   k_enstrophy  0.5|curl u|^2 from the local velocity field
 //   k_shift3     shift-only stencil of SRC/do_somethingGPU.F90:37-100
-#include <cstdlib>
-
 #include "kernels.h"
 #include "reduce.cuh"
 
@@ -441,137 +439,6 @@ __global__ void __launch_bounds__(128, ODD ? 5 : 6) k_aa_f16v(Pops<__half> a, Ge
   for (int q = 0; q < Q; ++q) {
     if (!ODD) *reinterpret_cast<uint2*>(a.p[oppq(q)] + row(0, 0) + i0) = Y[q];
     else shift_out(Y[q], cxq(q), a.p[q] + row_out(cyq(q), czq(q)), i0, i_prev, i_next, xl);
-  }
-}
-
-// The same AA steps as a persistent kernel with the source chunks of the next
-// work item copied into shared memory (cp.async, 8 bytes per thread and
-// population, plus the warp-edge lanes' crossing words) while the current one
-// is collided: the copies in flight hold no registers, so every warp keeps two
-// items' loads outstanding without losing occupancy. A work item is what one
-// 128-thread block of k_aa_f16v covers (the same thread -> cell mapping);
-// blocks take items round-robin. Each thread reads back only the shared-memory
-// slots it filled itself (the x-crossing values still move by shuffles), so no
-// block barrier is needed, and each (location, slot) pair is still read and
-// written only by the thread of the cell that owns it: copying the next
-// item's inputs before the current item's stores cannot race.
-constexpr int PIPE_NX = 10;  // populations with c_x != 0: q = 0..4 and 9..13
-struct PipeStage {
-  uint2 y[Q][128];             // the thread's aligned chunk of each source row
-  unsigned e[PIPE_NX][4][2];   // crossing words of lanes 0 and 31 of each warp
-};
-constexpr int PIPE_SMEM = 2 * (int)sizeof(PipeStage);
-
-__device__ __forceinline__ int pipe_eidx(int q) { return q < 5 ? q : q - 4; }
-
-__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((unsigned)__cvta_generic_to_shared(smem)),
-               "l"(gmem)
-               : "memory");
-}
-__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((unsigned)__cvta_generic_to_shared(smem)),
-               "l"(gmem)
-               : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
-
-// Cell coordinates of this thread in work item `item` (x-blocks of 128
-// threads over the ny * tpr threads of a plane, then planes).
-struct PipeCell {
-  int j, k, pos, i0;
-  bool valid;
-  __device__ PipeCell(long long item, int items_x, int log_tpr, const Geo& g) {
-    const int bx = (int)(item % items_x);
-    k = (int)(item / items_x);
-    const int t = bx * 128 + threadIdx.x;
-    j = t >> log_tpr;
-    pos = t & ((1 << log_tpr) - 1);
-    i0 = pos * 4;
-    valid = j < g.ny;  // whole warps: ny * tpr is a multiple of 32
-  }
-};
-
-template <bool ODD>
-__device__ __forceinline__ void pipe_issue(PipeStage& st, const Pops<__half>& a, const Geo& g, const PipeCell& c,
-                                           int tpr, const XLanes& xl) {
-  if (c.valid) {
-    const int jm = c.j == 0 ? g.ny - 1 : c.j - 1, jp = c.j == g.ny - 1 ? 0 : c.j + 1;
-    const int km = c.k == 0 ? g.nz - 1 : c.k - 1, kp = c.k == g.nz - 1 ? 0 : c.k + 1;
-    const int i_prev = c.pos == 0 ? g.nx - 1 : c.i0 - 1;  // odd: the high half of the word at i_prev - 1
-    const int i_next = c.pos == tpr - 1 ? 0 : c.i0 + 4;   // even: the low half of the word at i_next
-    const int w = threadIdx.x >> 5;
-#pragma unroll
-    for (int q = 0; q < Q; ++q) {
-      const int dy = ODD ? -cyq(q) : 0, dz = ODD ? -czq(q) : 0;
-      const int jj = dy > 0 ? jp : (dy < 0 ? jm : c.j);
-      const int kk = dz > 0 ? kp : (dz < 0 ? km : c.k);
-      const __half* p = a.p[ODD ? oppq(q) : q] + g.sx * (jj + g.ny * kk);
-      cp_async8(&st.y[q][threadIdx.x], p + c.i0);
-      if (ODD && cxq(q) > 0 && xl.edge_prev) cp_async4(&st.e[pipe_eidx(q)][w][0], p + (i_prev - 1));
-      if (ODD && cxq(q) < 0 && xl.edge_next) cp_async4(&st.e[pipe_eidx(q)][w][1], p + i_next);
-    }
-  }
-  cp_async_commit();
-}
-
-template <bool ODD, bool LES>
-__global__ void __launch_bounds__(128, 5) k_aa_f16v_pipe(Pops<__half> a, Geo g, StepK K, int log_tpr, int items_x,
-                                                         long long nitems) {
-  extern __shared__ __align__(16) unsigned char pipe_smem[];
-  PipeStage* stage = reinterpret_cast<PipeStage*>(pipe_smem);
-  const int tpr = 1 << log_tpr;
-  long long item = blockIdx.x;
-  int s = 0;
-  if (item < nitems) {
-    const PipeCell c(item, items_x, log_tpr, g);
-    pipe_issue<ODD>(stage[0], a, g, c, tpr, XLanes(tpr, c.pos, threadIdx.x & 31));
-  }
-  for (; item < nitems; item += gridDim.x, s ^= 1) {
-    const long long nxt = item + gridDim.x;
-    if (nxt < nitems) {
-      const PipeCell cn(nxt, items_x, log_tpr, g);
-      pipe_issue<ODD>(stage[s ^ 1], a, g, cn, tpr, XLanes(tpr, cn.pos, threadIdx.x & 31));
-      cp_async_wait<1>();
-    } else {
-      cp_async_wait<0>();
-    }
-    const PipeCell c(item, items_x, log_tpr, g);
-    if (!c.valid) continue;
-    const XLanes xl(tpr, c.pos, threadIdx.x & 31);
-    const int w = threadIdx.x >> 5;
-    uint2 Y[Q];
-#pragma unroll
-    for (int q = 0; q < Q; ++q) Y[q] = stage[s].y[q][threadIdx.x];
-    if (ODD) {
-      unsigned short E[Q];
-#pragma unroll
-      for (int q = 0; q < Q; ++q) {
-        E[q] = 0;
-        if (cxq(q) > 0 && xl.edge_prev) E[q] = (unsigned short)(stage[s].e[pipe_eidx(q)][w][0] >> 16);
-        if (cxq(q) < 0 && xl.edge_next) E[q] = (unsigned short)(stage[s].e[pipe_eidx(q)][w][1] & 0xffffu);
-      }
-      shift_rows(Y, E, xl);
-    }
-    collide4_f16<LES>(Y, K);
-    int js = c.j, ks = c.k;  // store rows recomputed after the collision
-    asm volatile("" : "+r"(js), "+r"(ks));
-    const int jms = js == 0 ? g.ny - 1 : js - 1, jps = js == g.ny - 1 ? 0 : js + 1;
-    const int kms = ks == 0 ? g.nz - 1 : ks - 1, kps = ks == g.nz - 1 ? 0 : ks + 1;
-    const int i_prev = c.pos == 0 ? g.nx - 1 : c.i0 - 1;
-    const int i_next = c.pos == tpr - 1 ? 0 : c.i0 + 4;
-#pragma unroll
-    for (int q = 0; q < Q; ++q) {
-      const int dy = ODD ? cyq(q) : 0, dz = ODD ? czq(q) : 0;
-      const int jj = dy > 0 ? jps : (dy < 0 ? jms : js);
-      const int kk = dz > 0 ? kps : (dz < 0 ? kms : ks);
-      if (!ODD) *reinterpret_cast<uint2*>(a.p[oppq(q)] + g.sx * (jj + g.ny * kk) + c.i0) = Y[q];
-      else shift_out(Y[q], cxq(q), a.p[q] + g.sx * (jj + g.ny * kk), c.i0, i_prev, i_next, xl);
-    }
   }
 }
 
@@ -1157,24 +1024,6 @@ static cudaError_t aa_impl(const Lattice& a, int odd, const StepK& K, int varian
   // FP16: four cells per thread where the box fits it (automatic or 4)
   if (lt4 >= 0) {
     const dim3 grid = f16v_grid(a.g, lt4, a.g.nz);
-    static int var = -1;
-    if (var < 0) {
-      const char* e = getenv("BGK_AA_PIPE");
-      var = e ? atoi(e) : 0;
-    }
-    if ((var & 1) && odd || (var & 2) && !odd) {
-      int dev = 0, nsm = 148, bps = 1;
-      cudaGetDevice(&dev);
-      cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-      auto kern = odd ? k_aa_f16v_pipe<true, false> : k_aa_f16v_pipe<false, false>;
-      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, PIPE_SMEM);
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, 128, PIPE_SMEM);
-      const long long nitems = (long long)grid.x * grid.y;
-      long long nb = (long long)nsm * (bps > 0 ? bps : 1);
-      if (nb > nitems) nb = nitems;
-      kern<<<(unsigned)nb, 128, PIPE_SMEM, st>>>(pops_of<__half>(a), a.g, K, lt4, (int)grid.x, nitems);
-      return cudaGetLastError();
-    }
     if (odd) k_aa_f16v<true, false><<<grid, 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
     else k_aa_f16v<false, false><<<grid, 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
     return cudaGetLastError();

@@ -554,6 +554,12 @@ def run_slabs(a):
         ms = float(t.item())
     launches = sum(b.launch_count for b in boxes) - l0
     clk = clocks.stop()
+    # the edge-plane kernel of the last step (device events), slowest slab
+    edge_us = max(b.slab_edge_time_us() for b in boxes)
+    if ws > 1:
+        t = torch.tensor([edge_us], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        edge_us = float(t.item())
     value = cells * a.steps / (ms * 1e-3) / 1e9
     bpc = BYTES_PER_CELL[a.precision]
     peak, peak_kind = measured_hbm()
@@ -572,7 +578,11 @@ def run_slabs(a):
                          "kernel": f"k_slab_{a.precision}", "per": "whole step of this GPU's slabs"},
             "exchange": {"bytes_per_step_per_gpu": exch, "peer": ws > 1,
                          "what": "2 faces x 5 populations x lx*ly x element size per slab, stored by the edge "
-                                 "kernel into the neighbours' ghost planes"},
+                                 "kernel into the neighbours' ghost planes",
+                         "edge_kernel_us": edge_us, "edge_share_of_step": edge_us * 1e-3 / (ms / a.steps),
+                         "edge_kernel_note": "device time of the last step's edge-plane kernel (boundary planes "
+                                             "and their peer stores), running beside the interior kernel; "
+                                             "slowest slab"},
             "cpu_baseline": None, "e2e": None, "gpu_launches": launches, "clocks": clk,
         }
         print(json.dumps(line), flush=True)

@@ -63,6 +63,7 @@ PROTOTYPES = [
     ("bgk_init_tgv", _i, [_vp]),
     ("bgk_init_velocity", _i, [_vp, _dp, _dp, _dp, _d]),
     ("bgk_init_velocity_device", _i, [_vp, _vp, _vp, _vp, _d]),
+    ("bgk_slab_edge_time", _i, [_vp, _dp]),
     ("bgk_boundaries", _i, [_vp, _i]),
     ("bgk_col_mc", _i, [_vp, _i]),
     ("bgk_run", _i, [_vp, _i]),

@@ -55,6 +55,9 @@ struct bgk_ctx {
   // z-slab: second stream for the interior planes and its fork / join events
   cudaStream_t st_in = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  // z-slab: timing events around the edge-plane kernel of each step
+  cudaEvent_t ev_edge0 = nullptr, ev_edge1 = nullptr;
+  int edge_timed = 0;
   Geo g{};
   size_t es = 8;
   void* memA = nullptr;
@@ -531,6 +534,8 @@ int bgk_create(const bgk_params* p, bgk_ctx** out) {
     e = cudaStreamCreateWithFlags(&c->st_in, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreate(&c->ev_edge0);
+    if (e == cudaSuccess) e = cudaEventCreate(&c->ev_edge1);
     if (e != cudaSuccess) return fail(cuda_fail(e, "slab stream"));
     e = cudaMemsetAsync(c->halo_mem, 0, c->halo_bytes, c->st);
     if (e != cudaSuccess) return fail(cuda_fail(e, "cudaMemset"));
@@ -567,6 +572,8 @@ int bgk_destroy(bgk_ctx* c) {
   if (c->mark) cudaEventDestroy(c->mark);
   if (c->ev_fork) cudaEventDestroy(c->ev_fork);
   if (c->ev_join) cudaEventDestroy(c->ev_join);
+  if (c->ev_edge0) cudaEventDestroy(c->ev_edge0);
+  if (c->ev_edge1) cudaEventDestroy(c->ev_edge1);
   if (c->st_in) cudaStreamDestroy(c->st_in);
   if (c->st) cudaStreamDestroy(c->st);
   delete c;
@@ -625,7 +632,11 @@ int bgk_col_mc(bgk_ctx* c, int itime) {
     const SlabLinks l = slab_links(c, (int)(c->step & 1), (int)((c->step + 1) & 1));
     CK(cudaEventRecord(c->ev_fork, c->st));
     CK(cudaStreamWaitEvent(c->st_in, c->ev_fork, 0));
+    // the edge-plane kernel is the only work on st between these two events
+    CK(cudaEventRecord(c->ev_edge0, c->st));
     CK(launch_slab(c->A, c->B, l, c->omega, c->scale, c->p.les_cs, c->st, c->st_in));
+    CK(cudaEventRecord(c->ev_edge1, c->st));
+    c->edge_timed = 1;
     CK(cudaEventRecord(c->ev_join, c->st_in));
     CK(cudaStreamWaitEvent(c->st, c->ev_join, 0));
     if (c->g.nz > 2) c->launches++;  // edge planes and interior are two launches
@@ -724,6 +735,25 @@ int bgk_halo_connect(bgk_ctx* c, void* below, void* above) {
   c->nb_below = below;
   c->nb_above = above;
   c->primed = 0;
+  return BGK_OK;
+}
+
+int bgk_slab_edge_time(bgk_ctx* c, double* us) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!us || !c->slab) {
+    set_err("bgk_slab_edge_time: null argument or not a z-slab context");
+    return BGK_ERR_INVALID;
+  }
+  if (!c->edge_timed) {
+    set_err("bgk_slab_edge_time: no step has run on this slab yet");
+    return BGK_ERR_STATE;
+  }
+  CK(cudaSetDevice(c->p.device));
+  CK(cudaEventSynchronize(c->ev_edge1));
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, c->ev_edge0, c->ev_edge1));
+  *us = 1e3 * (double)ms;
   return BGK_OK;
 }
 

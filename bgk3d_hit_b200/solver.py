@@ -283,6 +283,12 @@ class BGK3D:
     def halo_prime(self):
         check(self._lib.bgk_halo_prime(self._h), "bgk_halo_prime")
 
+    def slab_edge_time_us(self) -> float:
+        """Device time of the last step's edge-plane kernel (z-slab)."""
+        v = C.c_double()
+        check(self._lib.bgk_slab_edge_time(self._h, C.byref(v)), "bgk_slab_edge_time")
+        return v.value
+
 
 def fortran_e(x: float) -> str:
     """Fortran E14.6 edit descriptor (0.ddddddE+ee, right-justified), the

@@ -314,6 +314,14 @@ int bgk_halo_connect(bgk_ctx* ctx, void* below, void* above);
    the current step (after an initial condition, upload or restart). */
 int bgk_halo_prime(bgk_ctx* ctx);
 
+/* Duration in microseconds of the last step's edge-plane kernel of a z-slab
+   (the boundary planes that read the ghost planes and store into the
+   neighbours'), timed on the device with events while the interior kernel
+   runs beside it on the context's second stream. Waits for that step.
+   BGK_ERR_STATE before the slab's first step. No reference counterpart (the
+   reference's timers, SRC/finalize.F90:58-63, time its MPI exchange). */
+int bgk_slab_edge_time(bgk_ctx* ctx, double* us);
+
 /* Streaming-only calibrator, the single-box equivalent of do_somethingGPU
    (SRC/do_somethingGPU.F90:37-100) without the MPI barrier: out1(i,j,k) =
    in1(i-1,j,k), out2 = in2(i,j-1,k), out3 = in3(i,j,k-1) with periodic wrap

@@ -143,6 +143,29 @@ def test_slab_call_order_and_unsupported_calls(bgk):
     w.close()
 
 
+def test_slab_edge_kernel_time(bgk):
+    """The edge-plane kernel of a slab step is timed on the device: an error
+    before the first step, a positive duration shorter than the whole step
+    after it, and an error on a whole-box context."""
+    from bgk3d_hit_b200.slabs import LocalSlabs
+
+    sl = LocalSlabs(64, 64, 64, 2, svisc=0.01, u0=0.05, icheck=1)
+    try:
+        sl.init()
+        with pytest.raises(bgk.BgkError):
+            sl.slabs[0].slab_edge_time_us()
+        sl.run(3)
+        for s in sl.slabs:
+            us = s.slab_edge_time_us()
+            assert 0.0 < us < 1e5
+    finally:
+        sl.close()
+    w = bgk.BGK3D(8)
+    with pytest.raises(bgk.BgkError):
+        w.slab_edge_time_us()
+    w.close()
+
+
 def _two_process_worker(rank, port, out_dir, steps):
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     import datetime

@@ -25,8 +25,6 @@
 // Kernels run a fixed grid (DIAG_BLOCKS x DIAG_THREADS) striding over the
 // cells, and accumulate their sums into one compensated pair per block, so
 // repeated runs give identical bits.
-#include <cstdlib>
-
 #include "kernels.h"
 #include "reduce.cuh"
 
@@ -107,8 +105,8 @@ __global__ void __launch_bounds__(DIAG_THREADS) k_adj_terminal(Pops<const typena
 // added to the block's sum in double. Each block adds its dL/domega
 // contribution (warp shuffles, then the four warp sums in order) into its
 // own compensated pair acc[2*block].
-template <class F, int MINB = 4>
-__global__ void __launch_bounds__(128, MINB) k_adj_step(Pops<const typename F::S> ft, Pops<const typename F::S> lin,
+template <class F>
+__global__ void __launch_bounds__(128, 4) k_adj_step(Pops<const typename F::S> ft, Pops<const typename F::S> lin,
                                                      Pops<typename F::S> lout, Geo g, typename F::R omega,
                                                      double* acc) {
   using S = typename F::S; using R = typename F::R;
@@ -370,27 +368,11 @@ cudaError_t launch_adj_step(const Lattice& ft, const Lattice& lin, const Lattice
                             cudaStream_t st) {
   dim3 grid, block;
   adj_shape(ft.g, &grid, &block);
-  static int mb = -1;
-  if (mb < 0) {
-    const char* e = getenv("BGK_ADJ_MINB");
-    mb = e ? atoi(e) : 4;
-  }
-  switch (ft.form) {
-    case FORM_F64: {
-      auto a = pops<const double>(ft); auto b = pops<const double>(lin); auto c = pops<double>(lout);
-      if (mb == 5) k_adj_step<F64, 5><<<grid, block, 0, st>>>(a, b, c, ft.g, omega, acc);
-      else if (mb == 6) k_adj_step<F64, 6><<<grid, block, 0, st>>>(a, b, c, ft.g, omega, acc);
-      else k_adj_step<F64, 4><<<grid, block, 0, st>>>(a, b, c, ft.g, omega, acc);
-      return cudaGetLastError();
-    }
-    case FORM_F32: {
-      auto a = pops<const float>(ft); auto b = pops<const float>(lin); auto c = pops<float>(lout);
-      if (mb == 6) k_adj_step<F32, 6><<<grid, block, 0, st>>>(a, b, c, ft.g, (float)omega, acc);
-      else k_adj_step<F32, 4><<<grid, block, 0, st>>>(a, b, c, ft.g, (float)omega, acc);
-      return cudaGetLastError();
-    }
-  }
-  return cudaErrorInvalidValue;
+  BGK_FORM_DISPATCH(ft,
+      (k_adj_step<F64><<<grid, block, 0, st>>>(pops<const double>(ft), pops<const double>(lin), pops<double>(lout),
+                                               ft.g, omega, acc)),
+      (k_adj_step<F32><<<grid, block, 0, st>>>(pops<const float>(ft), pops<const float>(lin), pops<float>(lout),
+                                               ft.g, (float)omega, acc)))
 }
 
 cudaError_t launch_acc_total_n(const double* acc, long long n, double* total, cudaStream_t st) {

@@ -182,3 +182,30 @@ def test_bench_reference_arm_line_on_cpu():
         assert k in line, k
     assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["cores"] >= 1
     assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["value"] == line["value"]
+
+
+def test_bench_kernel_names_and_shared_config():
+    """The bench names the stream-collide kernel each run launches (the key of
+    its ncu traffic table) and both arms print the same config dict."""
+    import argparse
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path.insert(0, root)
+    import bench
+
+    assert bench.kernel_key("fp64", "two_lattice", 256) == "k_two_fp64"
+    assert bench.kernel_key("fp16", "two_lattice", 256) == "k_two_f16v"
+    assert bench.kernel_key("fp16", "two_lattice", 256, kernel=2) == "k_two_f16v2"
+    assert bench.kernel_key("fp16", "aa", 1024) == "k_aa_f16v"
+    assert bench.kernel_key("fp16", "two_lattice", 256, les=True) == "k_two_f16v_les"
+    assert bench.kernel_key("fp16", "aa", 256, les=True) == "k_aa_f16v_les"
+    assert bench.kernel_key("fp16", "two_lattice", 256, kernel=1) == "k_two_fp16"
+    assert bench.kernel_key("fp16", "two_lattice", 6) == "k_two_fp16"  # rows too short for four cells per thread
+    a = argparse.Namespace(size=256, precision="fp64", scheme="two_lattice", tau=0.505, k0=4.0, kernel=0, les_cs=0.0,
+                           decomp="replicas", local_slabs=2)
+    c1 = bench.config_of(a, 1)
+    assert c1["box"] == 256 and c1["cells_per_gpu"] == 256 ** 3 and "replica" in c1["parallelism"]
+    a.decomp = "slabs"
+    c4 = bench.config_of(a, 4)
+    assert c4["box"] == [256, 256, 1024] and c4["slabs"] == 4

@@ -11,6 +11,8 @@
 //                per-block partials
 //   k_enstrophy  0.5|curl u|^2 from the local velocity field
 //   k_shift3     shift-only stencil of SRC/do_somethingGPU.F90:37-100
+#include <cstdlib>
+
 #include "kernels.h"
 #include "reduce.cuh"
 
@@ -219,8 +221,8 @@ __device__ __forceinline__ void shift_out(uint2 Y, int cx, __half* p, int i0, in
   }
 }
 
-template <bool LES>
-__global__ void __launch_bounds__(128, 6) k_two_f16v(Pops<const __half> src, Pops<__half> dst, Geo g, StepK K,
+template <bool LES, int MINB = 6>
+__global__ void __launch_bounds__(128, MINB) k_two_f16v(Pops<const __half> src, Pops<__half> dst, Geo g, StepK K,
                                                   int log_tpr, int k0) {
   const int tpr = 1 << log_tpr;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -391,8 +393,8 @@ __global__ void __launch_bounds__(256, 5) k_aa_f16_odd(Pops<__half> a, Geo g, St
 // 62.8-65.0 with two cells per thread on the odd step, and 58 for one cell per
 // thread. The LES odd step recomputes its store rows the same way (96 registers,
 // a few spilled bytes, 5 blocks per SM).
-template <bool ODD, bool LES>
-__global__ void __launch_bounds__(128, ODD ? 5 : 6) k_aa_f16v(Pops<__half> a, Geo g, StepK K, int log_tpr) {
+template <bool ODD, bool LES, int MINB = (ODD ? 5 : 6)>
+__global__ void __launch_bounds__(128, MINB) k_aa_f16v(Pops<__half> a, Geo g, StepK K, int log_tpr) {
   const int tpr = 1 << log_tpr;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = t >> log_tpr, pos = t & (tpr - 1);
@@ -919,6 +921,23 @@ static dim3 f16v_grid(const Geo& g, int log_tpr, int planes) {
 }
 
 // log2(nx/V) when the V-cells-per-thread FP16 kernel applies, else -1.
+static int les_minb() {
+  static int v = -1;
+  if (v < 0) {
+    const char* e = getenv("BGK_LES_MINB");
+    v = e ? atoi(e) : 6;
+  }
+  return v;
+}
+static int bgk_minb() {
+  static int v = -1;
+  if (v < 0) {
+    const char* e = getenv("BGK_F16_MINB");
+    v = e ? atoi(e) : 6;
+  }
+  return v;
+}
+
 static int f16v_log_tpr(const Geo& g, int V) {
   if (g.nx % V) return -1;
   const int tpr = g.nx / V;
@@ -942,7 +961,8 @@ static cudaError_t two_impl(const Lattice& s, const Lattice& d, const StepK& K, 
       Pops<__half> ph = pops_of<__half>(d);
       ph.p[Q - 1] = (__half*)s.p[Q - 1];
       const dim3 grid = f16v_grid(s.g, lt, s.g.nz);
-      k_two_f16v<true><<<grid, 128, 0, st>>>(pops_of<const __half>(s), ph, s.g, K, lt, 0);
+      if (les_minb() == 5) k_two_f16v<true, 5><<<grid, 128, 0, st>>>(pops_of<const __half>(s), ph, s.g, K, lt, 0);
+      else k_two_f16v<true><<<grid, 128, 0, st>>>(pops_of<const __half>(s), ph, s.g, K, lt, 0);
     } else {
       k_two<F, true><<<sh.grid, sh.block, 0, st>>>(ps, pd, s.g, K);
     }
@@ -965,7 +985,8 @@ static cudaError_t two_impl(const Lattice& s, const Lattice& d, const StepK& K, 
       dim3 grid((unsigned)((threads + (V == 4 ? 127 : 255)) / (V == 4 ? 128 : 256)), s.g.nz);
       Pops<__half> ph = pops_of<__half>(d);
       ph.p[Q - 1] = (__half*)s.p[Q - 1];
-      if (V == 4) k_two_f16v<false><<<grid, 128, 0, st>>>(pops_of<const __half>(s), ph, s.g, K, lt, 0);
+      if (V == 4 && bgk_minb() == 5) k_two_f16v<false, 5><<<grid, 128, 0, st>>>(pops_of<const __half>(s), ph, s.g, K, lt, 0);
+      else if (V == 4) k_two_f16v<false><<<grid, 128, 0, st>>>(pops_of<const __half>(s), ph, s.g, K, lt, 0);
       else k_two_f16v2<<<grid, 256, 0, st>>>(pops_of<const __half>(s), ph, s.g, K, lt);
       return cudaGetLastError();
     }
@@ -1008,6 +1029,7 @@ static cudaError_t aa_impl(const Lattice& a, int odd, const StepK& K, int varian
     if (lt4 >= 0) {
       const dim3 grid = f16v_grid(a.g, lt4, a.g.nz);
       if (odd) k_aa_f16v<true, true><<<grid, 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
+      else if (les_minb() == 5) k_aa_f16v<false, true, 5><<<grid, 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
       else k_aa_f16v<false, true><<<grid, 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
     } else if (odd) {
       k_aa<F, true, true><<<sh.grid, sh.block, 0, st>>>(pops_of<S>(a), a.g, K);
@@ -1025,6 +1047,7 @@ static cudaError_t aa_impl(const Lattice& a, int odd, const StepK& K, int varian
   if (lt4 >= 0) {
     const dim3 grid = f16v_grid(a.g, lt4, a.g.nz);
     if (odd) k_aa_f16v<true, false><<<grid, 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
+    else if (bgk_minb() == 5) k_aa_f16v<false, false, 5><<<grid, 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
     else k_aa_f16v<false, false><<<grid, 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
     return cudaGetLastError();
   }

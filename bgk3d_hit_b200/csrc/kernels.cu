@@ -11,8 +11,6 @@
 //                per-block partials
 //   k_enstrophy  0.5|curl u|^2 from the local velocity field
 //   k_shift3     shift-only stencil of SRC/do_somethingGPU.F90:37-100
-#include <cstdlib>
-
 #include "kernels.h"
 #include "reduce.cuh"
 
@@ -92,10 +90,12 @@ __global__ void __launch_bounds__(256) k_two(Pops<const typename F::S> src, Pops
 // and 31 load it. Each cell's arithmetic is F16::cell's (moments16, pair16,
 // rest16). The collision runs on two cells at a time, their outputs replacing
 // their inputs in the packed registers, and the kernel runs 128-thread blocks
-// capped at 80 registers (6 blocks per SM, a few spilled bytes): on B200 at
-// 256^3 that measured 78.4-79.4 GLUPS, against 76.6 with 256-thread blocks at
-// the same cap, 64.5 for all four cells at once at 2 blocks per SM and 58.4
-// at 64 registers (heavy spills).
+// at 96 registers (5 blocks per SM, no spills). On B200 at 256^3, with every
+// row load issued before the shuffles, that measured 84.4 GLUPS against 82.0
+// capped at 80 registers (6 blocks per SM, 52 spilled bytes; the Smagorinsky
+// variant 78.5 against 67.9 with 108 spilled bytes); earlier forms of the
+// kernel measured 76.6 with 256-thread blocks, 64.5 for all four cells at once
+// at 2 blocks per SM and 58.4 at 64 registers (heavy spills).
 __device__ __forceinline__ unsigned short ldg_u16(const __half* p) {
   return __ldg(reinterpret_cast<const unsigned short*>(p));
 }
@@ -221,8 +221,8 @@ __device__ __forceinline__ void shift_out(uint2 Y, int cx, __half* p, int i0, in
   }
 }
 
-template <bool LES, int MINB = 6>
-__global__ void __launch_bounds__(128, MINB) k_two_f16v(Pops<const __half> src, Pops<__half> dst, Geo g, StepK K,
+template <bool LES>
+__global__ void __launch_bounds__(128, 5) k_two_f16v(Pops<const __half> src, Pops<__half> dst, Geo g, StepK K,
                                                   int log_tpr, int k0) {
   const int tpr = 1 << log_tpr;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -382,8 +382,8 @@ __global__ void __launch_bounds__(256, 5) k_aa_f16_odd(Pops<__half> a, Geo g, St
 // the store side. Every (location, slot) pair is still read and written by the
 // thread of the cell that owns it in the one-cell-per-thread kernel, or by a
 // lane of the same warp after a shuffle that orders it behind the owner's
-// loads, so the in-place update stays race-free. 128-thread blocks; the even
-// step is capped at 80 registers like k_two_f16v. The odd step stores to the
+// loads, so the in-place update stays race-free. 128-thread blocks at 96
+// registers (5 blocks per SM) like k_two_f16v. The odd step stores to the
 // rows it loaded from; left alone, the compiler keeps those 18 row addresses
 // live through the collision, so the BGK odd step recomputes them from an
 // opaque copy of (j, k) and fits 96 registers without spills (5 blocks per
@@ -391,10 +391,11 @@ __global__ void __launch_bounds__(256, 5) k_aa_f16_odd(Pops<__half> a, Geo g, St
 // with the addresses kept (128 registers, 4 blocks), 69.5 with 256-thread
 // blocks, 63.4 with the odd step capped at 80 registers (282 spilled bytes),
 // 62.8-65.0 with two cells per thread on the odd step, and 58 for one cell per
-// thread. The LES odd step recomputes its store rows the same way (96 registers,
-// a few spilled bytes, 5 blocks per SM).
-template <bool ODD, bool LES, int MINB = (ODD ? 5 : 6)>
-__global__ void __launch_bounds__(128, MINB) k_aa_f16v(Pops<__half> a, Geo g, StepK K, int log_tpr) {
+// thread; with the loads issued before the shuffles and the even step at 96
+// registers as well, 76.9. The LES odd step recomputes its store rows the
+// same way (96 registers, a few spilled bytes).
+template <bool ODD, bool LES>
+__global__ void __launch_bounds__(128, 5) k_aa_f16v(Pops<__half> a, Geo g, StepK K, int log_tpr) {
   const int tpr = 1 << log_tpr;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = t >> log_tpr, pos = t & (tpr - 1);
@@ -921,23 +922,6 @@ static dim3 f16v_grid(const Geo& g, int log_tpr, int planes) {
 }
 
 // log2(nx/V) when the V-cells-per-thread FP16 kernel applies, else -1.
-static int les_minb() {
-  static int v = -1;
-  if (v < 0) {
-    const char* e = getenv("BGK_LES_MINB");
-    v = e ? atoi(e) : 6;
-  }
-  return v;
-}
-static int bgk_minb() {
-  static int v = -1;
-  if (v < 0) {
-    const char* e = getenv("BGK_F16_MINB");
-    v = e ? atoi(e) : 6;
-  }
-  return v;
-}
-
 static int f16v_log_tpr(const Geo& g, int V) {
   if (g.nx % V) return -1;
   const int tpr = g.nx / V;
@@ -961,8 +945,7 @@ static cudaError_t two_impl(const Lattice& s, const Lattice& d, const StepK& K, 
       Pops<__half> ph = pops_of<__half>(d);
       ph.p[Q - 1] = (__half*)s.p[Q - 1];
       const dim3 grid = f16v_grid(s.g, lt, s.g.nz);
-      if (les_minb() == 5) k_two_f16v<true, 5><<<grid, 128, 0, st>>>(pops_of<const __half>(s), ph, s.g, K, lt, 0);
-      else k_two_f16v<true><<<grid, 128, 0, st>>>(pops_of<const __half>(s), ph, s.g, K, lt, 0);
+      k_two_f16v<true><<<grid, 128, 0, st>>>(pops_of<const __half>(s), ph, s.g, K, lt, 0);
     } else {
       k_two<F, true><<<sh.grid, sh.block, 0, st>>>(ps, pd, s.g, K);
     }
@@ -985,8 +968,7 @@ static cudaError_t two_impl(const Lattice& s, const Lattice& d, const StepK& K, 
       dim3 grid((unsigned)((threads + (V == 4 ? 127 : 255)) / (V == 4 ? 128 : 256)), s.g.nz);
       Pops<__half> ph = pops_of<__half>(d);
       ph.p[Q - 1] = (__half*)s.p[Q - 1];
-      if (V == 4 && bgk_minb() == 5) k_two_f16v<false, 5><<<grid, 128, 0, st>>>(pops_of<const __half>(s), ph, s.g, K, lt, 0);
-      else if (V == 4) k_two_f16v<false><<<grid, 128, 0, st>>>(pops_of<const __half>(s), ph, s.g, K, lt, 0);
+      if (V == 4) k_two_f16v<false><<<grid, 128, 0, st>>>(pops_of<const __half>(s), ph, s.g, K, lt, 0);
       else k_two_f16v2<<<grid, 256, 0, st>>>(pops_of<const __half>(s), ph, s.g, K, lt);
       return cudaGetLastError();
     }
@@ -1029,7 +1011,6 @@ static cudaError_t aa_impl(const Lattice& a, int odd, const StepK& K, int varian
     if (lt4 >= 0) {
       const dim3 grid = f16v_grid(a.g, lt4, a.g.nz);
       if (odd) k_aa_f16v<true, true><<<grid, 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
-      else if (les_minb() == 5) k_aa_f16v<false, true, 5><<<grid, 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
       else k_aa_f16v<false, true><<<grid, 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
     } else if (odd) {
       k_aa<F, true, true><<<sh.grid, sh.block, 0, st>>>(pops_of<S>(a), a.g, K);
@@ -1047,7 +1028,6 @@ static cudaError_t aa_impl(const Lattice& a, int odd, const StepK& K, int varian
   if (lt4 >= 0) {
     const dim3 grid = f16v_grid(a.g, lt4, a.g.nz);
     if (odd) k_aa_f16v<true, false><<<grid, 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
-    else if (bgk_minb() == 5) k_aa_f16v<false, false, 5><<<grid, 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
     else k_aa_f16v<false, false><<<grid, 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
     return cudaGetLastError();
   }

@@ -58,6 +58,10 @@ struct bgk_ctx {
   // z-slab: timing events around the edge-plane kernel of each step
   cudaEvent_t ev_edge0 = nullptr, ev_edge1 = nullptr;
   int edge_timed = 0;
+  // faithful two-lattice box: boundary planes of the states at the start of
+  // the last two steps (by step parity) and the step each one holds
+  void* faith_mem = nullptr;
+  long long faith_step[2] = {-1, -1};
   Geo g{};
   size_t es = 8;
   void* memA = nullptr;
@@ -296,7 +300,35 @@ int init_velocity_impl(bgk_ctx* c, const double* u, const double* v, const doubl
   c->lay = lay;
   c->step = 0;
   c->initialized = 1;
+  c->faith_step[0] = c->faith_step[1] = -1;
   c->primed = 0;
+  return BGK_OK;
+}
+
+// Faithful mode on a whole two-lattice box reproduces the ghost cells the
+// reference's dissipation pulls from: it runs after col_MC's pointer swap
+// (SRC/col_MC.F90:364-421, SRC/dissipation.F90:76-94), so after step t the
+// current lattice's ghosts hold the periodic images of the state at the
+// start of step t - 1 (its boundaries call), and after step 1 they were
+// never written (zero deviations, as a freshly allocated lattice). The
+// boundary planes of each step's starting state are kept by step parity.
+bool faith_on(const bgk_ctx* c) {
+  return c->p.mode == BGK_FAITHFUL && c->scheme == BGK_TWO_LATTICE && !c->slab;
+}
+
+void* faith_buf(const bgk_ctx* c, long long step) {
+  return (char*)c->faith_mem + (size_t)(step & 1) * (size_t)faith_planes_elems(c->g) * c->es;
+}
+
+int faith_snapshot(bgk_ctx* c) {
+  if (!faith_on(c)) return BGK_OK;
+  if (!c->faith_mem) {
+    int rc = dev_alloc(c, &c->faith_mem, 2 * (size_t)faith_planes_elems(c->g) * c->es, "faithful-mode ghost planes");
+    if (rc) return rc;
+  }
+  CK(launch_faith_snapshot(c->A, faith_buf(c, c->step), c->st));
+  c->launches++;
+  c->faith_step[c->step & 1] = c->step;
   return BGK_OK;
 }
 
@@ -307,8 +339,15 @@ int compute_diag(bgk_ctx* c, int itime, bgk_diag* out, int want_extras) {
     if (rc) return rc;
   }
   const SlabLinks hl = c->slab ? slab_links(c, (int)(c->step & 1), 0) : SlabLinks{};
+  const void* faith = nullptr;
+  bool faith_zero = false;
+  if (faith_on(c) && c->step == 1) {
+    faith_zero = true;
+  } else if (faith_on(c) && c->step >= 2 && c->faith_step[c->step & 1] == c->step - 2) {
+    faith = faith_buf(c, c->step);
+  }
   CK(launch_diag(c->A, c->lay, c->p.svisc, c->omega, c->scale, c->partials, extras ? c->vel : nullptr, c->st,
-                 c->slab ? &hl : nullptr));
+                 c->slab ? &hl : nullptr, faith, faith_zero));
   c->launches++;
   if (extras) {
     CK(launch_enstrophy(c->A, c->vel, c->partials, c->st));
@@ -565,6 +604,7 @@ int bgk_destroy(bgk_ctx* c) {
   for (void* m : c->lat_pool) cudaFree(m);
   for (void* m : c->ipc_maps) cudaIpcCloseMemHandle(m);
   cudaFree(c->halo_mem);
+  cudaFree(c->faith_mem);
   for (double* m : c->vel_pool) cudaFree(m);
   cudaFree(c->adj_acc);
   cudaFree(c->adj_tot);
@@ -599,6 +639,7 @@ int bgk_init_tgv(bgk_ctx* c) {
   c->lay = lay;
   c->step = 0;
   c->initialized = 1;
+  c->faith_step[0] = c->faith_step[1] = -1;
   c->primed = 0;
   return BGK_OK;
 }
@@ -641,6 +682,8 @@ int bgk_col_mc(bgk_ctx* c, int itime) {
     CK(cudaStreamWaitEvent(c->st, c->ev_join, 0));
     if (c->g.nz > 2) c->launches++;  // edge planes and interior are two launches
   } else if (c->scheme == BGK_TWO_LATTICE) {
+    rc = faith_snapshot(c);
+    if (rc) return rc;
     CK(launch_two_lattice(c->A, c->B, c->omega, c->scale, c->p.les_cs, c->p.kernel, c->st));
   }
   if (c->scheme == BGK_TWO_LATTICE) {
@@ -888,6 +931,7 @@ int bgk_put_populations(bgk_ctx* c, const void* host) {
   c->lay = lay;
   if (!c->initialized) c->step = 0;
   c->initialized = 1;
+  c->faith_step[0] = c->faith_step[1] = -1;
   c->primed = 0;
   return BGK_OK;
 }
@@ -1081,8 +1125,10 @@ int bgk_load(bgk_ctx* c, const char* path) {
   CK(cudaStreamSynchronize(c->st));
   c->lay = lay;
   c->step = h.step;
+  c->faith_step[0] = c->faith_step[1] = -1;
   if (c->form == FORM_F16) c->scale = h.scale;
   c->initialized = 1;
+  c->faith_step[0] = c->faith_step[1] = -1;
   c->primed = 0;
   return BGK_OK;
 }

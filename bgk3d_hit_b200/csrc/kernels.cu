@@ -690,10 +690,52 @@ __global__ void k_import(Pops<typename F::S> a, Geo g, int q, const typename F::
 // SRC/diagno.F90:96-111); 5 0.5|u|^2, 6 2*svisc*Ptotal (pulled populations,
 // SRC/dissipation.F90:76-249); 7 2*nu*S:S with S = -3*omega*Pi/(2*rho);
 // 8 non-finite cell count; 9 enstrophy (k_enstrophy).
+// Offset of the periodic image of an out-of-box source cell (si, sj, sk) in a
+// population's block of a boundary-plane snapshot: x planes (ny*nz each), then
+// y planes (nx*nz), then z planes (nx*ny).
+__device__ __forceinline__ long long faith_off(const Geo& g, int si, int sj, int sk) {
+  const int wi = wrapi(si, g.nx), wj = wrapi(sj, g.ny), wk = wrapi(sk, g.nz);
+  const long long yz = (long long)g.ny * g.nz, xz = (long long)g.nx * g.nz, xy = (long long)g.nx * g.ny;
+  if (si < 0 || si >= g.nx) return (wi == 0 ? 0 : yz) + wj + (long long)g.ny * wk;
+  if (sj < 0 || sj >= g.ny) return 2 * yz + (wj == 0 ? 0 : xz) + wi + (long long)g.nx * wk;
+  return 2 * (yz + xz) + (wk == 0 ? 0 : xy) + wi + (long long)g.nx * wj;
+}
+
+template <class S>
+__global__ void k_faith_snapshot(Pops<const S> a, Geo g, S* out) {
+  const long long yz = (long long)g.ny * g.nz, xz = (long long)g.nx * g.nz, xy = (long long)g.nx * g.ny;
+  const long long per = 2 * (yz + xz + xy), n = (long long)Q * per;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+    const int q = (int)(e / per);
+    long long r = e % per;
+    int i, j, k;
+    if (r < 2 * yz) {
+      i = r < yz ? 0 : g.nx - 1;
+      r %= yz;
+      j = (int)(r % g.ny);
+      k = (int)(r / g.ny);
+    } else if (r < 2 * (yz + xz)) {
+      r -= 2 * yz;
+      j = r < xz ? 0 : g.ny - 1;
+      r %= xz;
+      i = (int)(r % g.nx);
+      k = (int)(r / g.nx);
+    } else {
+      r -= 2 * (yz + xz);
+      k = r < xy ? 0 : g.nz - 1;
+      r %= xy;
+      i = (int)(r % g.nx);
+      j = (int)(r / g.nx);
+    }
+    out[e] = a.p[q][i + (long long)g.sx * (j + (long long)g.ny * k)];
+  }
+}
+
 template <class F, int LAY>
 __global__ void __launch_bounds__(DIAG_THREADS) k_diag(Pops<const typename F::S> a, Geo g, double svisc,
                                                        double omega, typename F::R inv, double* partials,
-                                                       typename F::R* vel, Halo<typename F::S> h) {
+                                                       typename F::R* vel, Halo<typename F::S> h,
+                                                       const typename F::S* __restrict__ faith, int faith_zero) {
   using R = typename F::R; using V = typename F::V; using N = Num<V>;
   __shared__ KS sh[DIAG_THREADS];
   KS acc[ND];
@@ -722,9 +764,16 @@ __global__ void __launch_bounds__(DIAG_THREADS) k_diag(Pops<const typename F::S>
     for (int q = 0; q < Q; ++q) {
       // a z-slab pulls across its faces from its ghost planes
       const bool lo = czq(q) > 0 && k == 0, hi = czq(q) < 0 && k == g.nz - 1;
+      const int si = i - cxq(q), sj = j - cyq(q), sk = k - czq(q);
       if (LAY == LAY_TWO && h.in_lo[0] && (lo || hi)) {
         const int po = wrapi(i - cxq(q), g.nx) + g.sx * wrapi(j - cyq(q), g.ny);
         x[q] = N::wrap(F::dec(lo ? h.in_lo[zslot(q)][po] : h.in_hi[zslot(q)][po], inv));
+      } else if (LAY == LAY_TWO && (faith || faith_zero) &&
+                 (si < 0 || si >= g.nx || sj < 0 || sj >= g.ny || sk < 0 || sk >= g.nz)) {
+        // faithful mode: the reference's ghost cell of this pull, filled two
+        // steps earlier (or never)
+        const long long per = 2 * ((long long)g.ny * g.nz + (long long)g.nx * g.nz + (long long)g.nx * g.ny);
+        x[q] = faith_zero ? N::c(0.0) : N::wrap(F::dec(faith[q * per + faith_off(g, si, sj, sk)], inv));
       } else {
         x[q] = N::wrap(F::dec(a.p[ref_slot<LAY>(q)][ref_off<LAY>(g, q, i, j, k, -cxq(q), -cyq(q), -czq(q))], inv));
       }
@@ -1147,25 +1196,42 @@ template <class S> static Halo<S> halo_of(const SlabLinks* l) {
 
 template <class F, int LAY>
 static void diag_lay(const Lattice& a, double svisc, double omega, double scale, double* partials, void* vel,
-                     const SlabLinks* halo, cudaStream_t st) {
+                     const SlabLinks* halo, const void* faith, bool fzero, cudaStream_t st) {
   using S = typename F::S; using R = typename F::R;
   k_diag<F, LAY><<<DIAG_BLOCKS, DIAG_THREADS, 0, st>>>(pops_of<const S>(a), a.g, svisc, omega, (R)(1.0 / scale),
-                                                       partials, (R*)vel, halo_of<S>(halo));
+                                                       partials, (R*)vel, halo_of<S>(halo), (const S*)faith,
+                                                       fzero ? 1 : 0);
 }
 template <class F>
 static cudaError_t diag_impl(const Lattice& a, int lay, double svisc, double omega, double scale, double* partials,
-                             void* vel, const SlabLinks* halo, cudaStream_t st) {
-  if (lay == LAY_TWO) diag_lay<F, LAY_TWO>(a, svisc, omega, scale, partials, vel, halo, st);
-  else if (lay == LAY_AAE) diag_lay<F, LAY_AAE>(a, svisc, omega, scale, partials, vel, halo, st);
-  else diag_lay<F, LAY_AAN>(a, svisc, omega, scale, partials, vel, halo, st);
+                             void* vel, const SlabLinks* halo, const void* faith, bool fzero, cudaStream_t st) {
+  if (lay == LAY_TWO) diag_lay<F, LAY_TWO>(a, svisc, omega, scale, partials, vel, halo, faith, fzero, st);
+  else if (lay == LAY_AAE) diag_lay<F, LAY_AAE>(a, svisc, omega, scale, partials, vel, halo, nullptr, false, st);
+  else diag_lay<F, LAY_AAN>(a, svisc, omega, scale, partials, vel, halo, nullptr, false, st);
+  return cudaGetLastError();
+}
+
+long long faith_planes_elems(const Geo& g) {
+  return (long long)Q * 2 * ((long long)g.ny * g.nz + (long long)g.nx * g.nz + (long long)g.nx * g.ny);
+}
+
+cudaError_t launch_faith_snapshot(const Lattice& a, void* out, cudaStream_t st) {
+  const long long n = faith_planes_elems(a.g);
+  const int blocks = grid_1d(n, 256, 148 * 16);
+  switch (a.form) {
+    case FORM_F64: k_faith_snapshot<double><<<blocks, 256, 0, st>>>(pops_of<const double>(a), a.g, (double*)out); break;
+    case FORM_F32: k_faith_snapshot<float><<<blocks, 256, 0, st>>>(pops_of<const float>(a), a.g, (float*)out); break;
+    case FORM_F16: k_faith_snapshot<__half><<<blocks, 256, 0, st>>>(pops_of<const __half>(a), a.g, (__half*)out); break;
+    default: return cudaErrorInvalidValue;
+  }
   return cudaGetLastError();
 }
 cudaError_t launch_diag(const Lattice& a, int lay, double svisc, double omega, double scale, double* partials,
-                        void* vel, cudaStream_t st, const SlabLinks* halo) {
+                        void* vel, cudaStream_t st, const SlabLinks* halo, const void* faith, bool faith_zero) {
   switch (a.form) {
-    case FORM_F64: return diag_impl<F64>(a, lay, svisc, omega, scale, partials, vel, halo, st);
-    case FORM_F32: return diag_impl<F32>(a, lay, svisc, omega, scale, partials, vel, halo, st);
-    case FORM_F16: return diag_impl<F16>(a, lay, svisc, omega, scale, partials, vel, halo, st);
+    case FORM_F64: return diag_impl<F64>(a, lay, svisc, omega, scale, partials, vel, halo, faith, faith_zero, st);
+    case FORM_F32: return diag_impl<F32>(a, lay, svisc, omega, scale, partials, vel, halo, faith, faith_zero, st);
+    case FORM_F16: return diag_impl<F16>(a, lay, svisc, omega, scale, partials, vel, halo, faith, faith_zero, st);
   }
   return cudaErrorInvalidValue;
 }

@@ -95,11 +95,21 @@ cudaError_t launch_export(const Lattice& a, int lay, int q, void* dense_stored, 
                           cudaStream_t st);
 cudaError_t launch_import(const Lattice& a, int lay, int q, const void* dense_stored, cudaStream_t st);
 
+// Faithful-mode ghosts: the six boundary planes (x = 0, nx-1; y = 0, ny-1;
+// z = 0, nz-1) of every population of a two-lattice state, stored type,
+// population-major; faith_planes_elems is the size of one snapshot.
+long long faith_planes_elems(const Geo& g);
+cudaError_t launch_faith_snapshot(const Lattice& a, void* out, cudaStream_t st);
+
 // Diagnostics: per-block partial sums (Neumaier pairs) of ND quantities.
 // vel (optional, 3*N values of the arithmetic type) receives the local velocity.
 // halo: the ghost planes of a z-slab (in_lo / in_hi), nullptr for a whole box.
+// faith (two-lattice only): pulls that leave the box read the periodic image
+// from this boundary-plane snapshot instead of the current state; with
+// faith_zero they read a zero deviation (ghosts never written).
 cudaError_t launch_diag(const Lattice& a, int lay, double svisc, double omega, double scale, double* partials,
-                        void* vel, cudaStream_t st, const SlabLinks* halo = nullptr);
+                        void* vel, cudaStream_t st, const SlabLinks* halo = nullptr, const void* faith = nullptr,
+                        bool faith_zero = false);
 
 // z-slab two-lattice step (src -> dst, pop 19 in place) reading the ghost
 // planes links.in_* and storing the outgoing boundary populations into

@@ -64,7 +64,12 @@ extern "C" {
 #define BGK_CORRECTED 0 /* TGV init in double with rho = 1; diagno sums ztot */
 #define BGK_FAITHFUL 1  /* TGV init with single-precision coordinates, pi and the
                            pressure-consistent crho (SRC/init.F90:42,84-95);
-                           diagno keeps ztot = ytot + zj (SRC/diagno.F90:110) */
+                           diagno keeps ztot = ytot + zj (SRC/diagno.F90:110);
+                           on a whole two-lattice box, dissipation pulls the
+                           reference's stale ghost cells (it runs after the
+                           pointer swap: after step t >= 2 the ghosts hold the
+                           state of step t - 2, after step 1 zero deviations);
+                           sums stay compensated FP64 in both modes */
 
 typedef struct bgk_ctx bgk_ctx;
 
@@ -344,7 +349,9 @@ int bgk_shift3(const void* in1, const void* in2, const void* in3, void* out1, vo
    driver that keeps the reference's ghosted (0:l+1, 0:m+1, 0:n+1) arrays
    passes a copy of their interior, not the ghosted arrays themselves. svisc and omega enter the
    dissipation and strain sums, u0 and itime the dissipation.dat columns, mode
-   the diagno ztot convention. Runs on the calling thread's current device and
+   the diagno ztot convention (without a history of earlier states, its
+   dissipation pulls are periodic in both modes). Runs on the calling thread's
+   current device and
    on `stream` (NULL: default stream), then synchronises that stream.
    Scratch: one file-scope device array of 94,808 bytes per GPU (held until the
    process exits), whatever the box size; boxes are limited to

@@ -667,7 +667,10 @@ static inline REAL FN(ptotal)(const REAL x[19], const REAL e[19]) {
    (SRC/dissipation.F90:65-66).
    faithful=0: periodic pulls and compensated double sums (2*svisc*Ptotal and
    0.5*vsq are formed in REAL per cell, as in the reference, then summed in
-   double). */
+   double).
+   faithful=2: the stale ghost layers of faithful=1 with the compensated sums
+   of faithful=0 (the CUDA path's faithful mode, whose sums are compensated
+   in every mode). */
 void FN(orc_dissipation)(const LAT *L, double sviscd, double u0d, int itime, int faithful, double out[4]) {
     const long l = L->l, m = L->m, n = L->n;
     const REAL svisc = (REAL)sviscd, u0 = (REAL)u0d;
@@ -679,11 +682,11 @@ void FN(orc_dissipation)(const LAT *L, double sviscd, double u0d, int itime, int
         for (long j = 1; j <= m; ++j)
             for (long i = 1; i <= l; ++i) {
                 REAL x[19], e[19], ux, uy, uz;
-                FN(pull)(L, L->a, i, j, k, !faithful, x);
+                FN(pull)(L, L->a, i, j, k, faithful == 0, x);
                 (void)FN(equilibrium)(x, e, &ux, &uy, &uz);
                 REAL vsq = ux * ux + uy * uy + uz * uz;
                 REAL P = FN(ptotal)(x, e);
-                if (faithful) {
+                if (faithful == 1) {
                     tke = tke + (REAL)0.5 * vsq;
                     diss = diss + (REAL)2.0 * svisc * P;
                 } else {
@@ -691,7 +694,7 @@ void FN(orc_dissipation)(const LAT *L, double sviscd, double u0d, int itime, int
                     FN(kadd)(&kd, (double)((REAL)2.0 * svisc * P));
                 }
             }
-    if (faithful) {
+    if (faithful == 1) {
         out[0] = (double)((REAL)(float)itime * dt);
         out[1] = (double)(tke / (REAL)(float)l / (REAL)(float)m / (REAL)(float)n / (u0 * u0));
         out[2] = (double)diss;

@@ -162,7 +162,10 @@ class OracleLattice:
         self._f("orc_diagno")(self.h, int(faithful), _dptr(out))
         return out
 
-    def dissipation(self, svisc: float, u0: float, itime: int, faithful: bool = False) -> np.ndarray:
+    def dissipation(self, svisc: float, u0: float, itime: int, faithful: bool | int = False) -> np.ndarray:
+        """faithful: False/0 periodic pulls, compensated sums; True/1 stale
+        ghosts (the reference's), sequential sums; 2 stale ghosts, compensated
+        sums."""
         out = np.zeros(4)
         self._f("orc_dissipation")(self.h, svisc, u0, itime, int(faithful), _dptr(out))
         return out

@@ -172,36 +172,46 @@ def test_init_velocity_device_equals_host_init(bgk, form, scheme):
         b.close()
 
 
-def test_faithful_mode_dissipation_is_the_periodic_value(bgk, oracle_mod):
+@pytest.mark.parametrize("form", ["fp64", "fp32", "fp16"])
+def test_faithful_mode_dissipation_reads_the_reference_ghosts(bgk, oracle_mod, form):
     """The reference computes dissipation after col_MC's pointer swap
     (SRC/col_MC.F90:364-421, SRC/dissipation.F90:76-94), so its border cells
-    pull ghost values of the lattice that were filled two steps earlier, or
-    never (the second lattice's ghosts before its first boundaries call). The
-    GPU has no ghosts and computes the periodic value in both modes: here, on
-    the C1 box (TGV 64^3, faithful init, nu = 0.01), it equals the oracle's
-    periodic dissipation to 1e-12 while the oracle's stale-ghost (faithful)
-    value differs from it by 64x at step 1, ~1% at step 2, ~0.5% at step 10
-    and ~3e-5 at step 100 (asserted as ranges)."""
-    orc = oracle_mod.OracleLattice(64, 64, 64, form="f64")
+    pull ghost values filled two steps earlier, or never (the second lattice
+    before its first boundaries call). A faithful-mode two-lattice box
+    reproduces those pulls: on the C1 box (TGV 64^3, faithful init,
+    nu = 0.01) its diss / tke equal the oracle's stale-ghost values (stepped
+    with the step3 ghost fill, summed compensated) to 1e-12 at steps 1, 2, 10
+    and 100, where the stale-ghost artefact is 64x, ~1%, ~0.5% and ~3e-5 of
+    the periodic value; a corrected-mode box keeps the periodic value."""
+    F16 = 2.0 ** 16
+    forms = {"fp64": "f64", "fp32": "f32", "fp16": "f16"}
+    orc = oracle_mod.OracleLattice(64, 64, 64, form=forms[form], scale=F16)
     orc.init_tgv(0.05, faithful=True)
-    box = bgk.BGK3D(64, svisc=0.01, u0=0.05, precision="fp64", icheck=1, mode="faithful")
-    box.set_populations(orc.get_pops())
+    kw = dict(svisc=0.01, u0=0.05, precision=form, icheck=1, fp16_scale=F16 if form == "fp16" else 0.0)
+    faith = bgk.BGK3D(64, mode="faithful", **kw)
+    corr = bgk.BGK3D(64, mode="corrected", **kw)
+    for b in (faith, corr):
+        b.set_populations(orc.get_pops())
     gaps = {}
     try:
         for it in range(1, 101):
             orc.step(0.01)  # boundaries (ghost fill) + col_MC, as the reference loop
-            box.boundaries(it)
-            box.col_MC(it)
+            for b in (faith, corr):
+                b.boundaries(it)
+                b.col_MC(it)
             if it in (1, 2, 10, 100):
-                d = box.diagnostic(it)
-                per = orc.dissipation(0.01, 0.05, it, False)
-                stale = orc.dissipation(0.01, 0.05, it, True)
-                assert d["diss"] == pytest.approx(per[2], rel=1e-12)
-                assert d["tke_norm"] == pytest.approx(per[1], rel=1e-12)
+                stale = orc.dissipation(0.01, 0.05, it, 2)
+                per = orc.dissipation(0.01, 0.05, it, 0)
+                df, dc = faith.diagnostic(it), corr.diagnostic(it)
+                np.testing.assert_allclose([df["tke_norm"], df["diss"], df["tke"]], stale[1:], rtol=1e-12, err_msg=f"{it}")
+                np.testing.assert_allclose([dc["tke_norm"], dc["diss"], dc["tke"]], per[1:], rtol=1e-12, err_msg=f"{it}")
+                assert df["t"] == stale[0]
                 gaps[it] = abs(stale[2] - per[2]) / abs(per[2])
+        assert same_bits(faith.populations(), orc.get_pops())
     finally:
         orc.close()
-        box.close()
+        faith.close()
+        corr.close()
     assert gaps[1] > 10
     assert 1e-3 < gaps[2] < 1e-1 and 1e-3 < gaps[10] < 1e-1
     assert 1e-6 < gaps[100] < 1e-3

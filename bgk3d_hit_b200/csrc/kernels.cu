@@ -11,6 +11,8 @@
 //                per-block partials
 //   k_enstrophy  0.5|curl u|^2 from the local velocity field
 //   k_shift3     shift-only stencil of SRC/do_somethingGPU.F90:37-100
+#include <cstdlib>
+
 #include "kernels.h"
 #include "reduce.cuh"
 
@@ -394,13 +396,52 @@ __global__ void __launch_bounds__(256, 5) k_aa_f16_odd(Pops<__half> a, Geo g, St
 // thread; with the loads issued before the shuffles and the even step at 96
 // registers as well, 76.9. The LES odd step recomputes its store rows the
 // same way (96 registers, a few spilled bytes).
-template <bool ODD, bool LES>
+// Store side of the odd step when the x-crossing values of warp edges come
+// from the neighbouring warp of the same block through shared memory: an edge
+// lane whose neighbour warp is in the block stores a whole aligned 8-byte
+// chunk (the crossing element included) and the neighbour skips its 2-byte
+// store of that element; edges at block boundaries keep the partial stores
+// of shift_out. from_prev / from_next: the neighbour warp's crossing value.
+__device__ __forceinline__ void shift_out_blk(uint2 Y, int cx, __half* p, int i0, int i_prev, int i_next,
+                                              const XLanes& xl, bool prev_in, bool next_in, unsigned from_prev,
+                                              unsigned from_next) {
+  unsigned short* u = reinterpret_cast<unsigned short*>(p);
+  if (cx == 0) {
+    *reinterpret_cast<uint2*>(p + i0) = Y;
+  } else if (cx > 0) {  // cell i0+m -> element i0+m+1
+    unsigned prev = __shfl_sync(0xffffffffu, Y.y >> 16, xl.src_prev);  // cell i0-1 of the lane before
+    if (xl.edge_prev && prev_in) prev = from_prev;
+    const unsigned lo = __byte_perm(prev, Y.x, 0x5410), hi = __byte_perm(Y.x, Y.y, 0x5432);
+    if (!xl.edge_prev || prev_in) {
+      *reinterpret_cast<uint2*>(p + i0) = make_uint2(lo, hi);
+    } else {
+      u[i0 + 1] = (unsigned short)(Y.x & 0xffffu);
+      *reinterpret_cast<unsigned*>(p + i0 + 2) = hi;
+    }
+    if (xl.edge_next && !next_in) u[i_next] = (unsigned short)(Y.y >> 16);
+  } else {  // cell i0+m -> element i0+m-1
+    unsigned next = __shfl_sync(0xffffffffu, Y.x & 0xffffu, xl.src_next);  // cell i0+4 of the lane after
+    if (xl.edge_next && next_in) next = from_next;
+    const unsigned lo = __byte_perm(Y.x, Y.y, 0x5432), hi = __byte_perm(Y.y, next, 0x5432);
+    if (!xl.edge_next || next_in) {
+      *reinterpret_cast<uint2*>(p + i0) = make_uint2(lo, hi);
+    } else {
+      *reinterpret_cast<unsigned*>(p + i0) = lo;
+      u[i0 + 2] = (unsigned short)(Y.y >> 16);
+    }
+    if (xl.edge_prev && !prev_in) u[i_prev] = (unsigned short)(Y.x & 0xffffu);
+  }
+}
+
+template <bool ODD, bool LES, bool BLK = false>
 __global__ void __launch_bounds__(128, 5) k_aa_f16v(Pops<__half> a, Geo g, StepK K, int log_tpr) {
   const int tpr = 1 << log_tpr;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = t >> log_tpr, pos = t & (tpr - 1);
+  const int j0 = t >> log_tpr, pos = t & (tpr - 1);
   const int k = blockIdx.y;
-  if (j >= g.ny) return;  // whole warps: ny*tpr is a multiple of 32
+  const bool valid = j0 < g.ny;  // whole warps: ny*tpr is a multiple of 32
+  if (!(ODD && BLK) && !valid) return;
+  const int j = valid ? j0 : 0;  // an idle warp of the block-edge variant only reaches its barrier
   const XLanes xl(tpr, pos, threadIdx.x & 31);
   const int i0 = pos * 4;
   const int jm = j == 0 ? g.ny - 1 : j - 1, jp = j == g.ny - 1 ? 0 : j + 1;
@@ -413,7 +454,10 @@ __global__ void __launch_bounds__(128, 5) k_aa_f16v(Pops<__half> a, Geo g, StepK
     return g.sx * (jj + g.ny * kk);
   };
   uint2 Y[Q];
-  if (ODD) {
+  if (ODD && BLK && !valid) {
+#pragma unroll
+    for (int q = 0; q < Q; ++q) Y[q] = make_uint2(0u, 0u);
+  } else if (ODD) {
     unsigned short E[Q];
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
@@ -428,7 +472,40 @@ __global__ void __launch_bounds__(128, 5) k_aa_f16v(Pops<__half> a, Geo g, StepK
 #pragma unroll
     for (int q = 0; q < Q; ++q) Y[q] = __ldg(reinterpret_cast<const uint2*>(a.p[q] + row(0, 0) + i0));
   }
-  collide4_f16<LES>(Y, K);
+  if (!(ODD && BLK && !valid)) collide4_f16<LES>(Y, K);
+  // block-edge variant: the warps' crossing values (cx > 0 populations: the
+  // last lane's last cell; cx < 0: the first lane's first cell) through
+  // shared memory; the barrier also orders every warp's loads before any
+  // warp's stores of its neighbours' crossing elements
+  __shared__ unsigned xs_last[ODD && BLK ? 4 : 1][5], xs_first[ODD && BLK ? 4 : 1][5];
+  bool prev_in = false, next_in = false;
+  int wprev = 0, wnext = 0;
+  if (ODD && BLK) {
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (tpr >= 32) {
+      const int nw = tpr >> 5, r = pos >> 5;  // warps per row, this warp's place in its row
+      if (nw <= 4) {  // the whole row in this block
+        prev_in = next_in = true;
+        wprev = w - r + (r + nw - 1) % nw;
+        wnext = w - r + (r + 1) % nw;
+      } else {
+        prev_in = w > 0;
+        next_in = w < 3;
+        wprev = w - 1;
+        wnext = w + 1;
+      }
+      if (valid && lane == 31) {
+#pragma unroll
+        for (int q = 0; q < 5; ++q) xs_last[w][q] = Y[q].y >> 16;
+      }
+      if (valid && lane == 0) {
+#pragma unroll
+        for (int q = 9; q < 14; ++q) xs_first[w][q - 9] = Y[q].x & 0xffffu;
+      }
+    }
+    __syncthreads();
+    if (!valid) return;
+  }
   int js = j, ks = k;  // store rows: recomputed after the collision (BGK odd step)
   if (ODD) asm volatile("" : "+r"(js), "+r"(ks));
   const int jms = js == 0 ? g.ny - 1 : js - 1, jps = js == g.ny - 1 ? 0 : js + 1;
@@ -440,8 +517,16 @@ __global__ void __launch_bounds__(128, 5) k_aa_f16v(Pops<__half> a, Geo g, StepK
   };
 #pragma unroll
   for (int q = 0; q < Q; ++q) {
-    if (!ODD) *reinterpret_cast<uint2*>(a.p[oppq(q)] + row(0, 0) + i0) = Y[q];
-    else shift_out(Y[q], cxq(q), a.p[q] + row_out(cyq(q), czq(q)), i0, i_prev, i_next, xl);
+    if (!ODD) {
+      *reinterpret_cast<uint2*>(a.p[oppq(q)] + row(0, 0) + i0) = Y[q];
+    } else if (BLK) {
+      const unsigned fp = cxq(q) > 0 && xl.edge_prev && prev_in ? xs_last[wprev][q] : 0u;
+      const unsigned fn = cxq(q) < 0 && xl.edge_next && next_in ? xs_first[wnext][q - 9] : 0u;
+      shift_out_blk(Y[q], cxq(q), a.p[q] + row_out(cyq(q), czq(q)), i0, i_prev, i_next, xl, prev_in, next_in, fp,
+                    fn);
+    } else {
+      shift_out(Y[q], cxq(q), a.p[q] + row_out(cyq(q), czq(q)), i0, i_prev, i_next, xl);
+    }
   }
 }
 
@@ -1059,7 +1144,13 @@ static cudaError_t aa_impl(const Lattice& a, int odd, const StepK& K, int varian
   if (K.les) {
     if (lt4 >= 0) {
       const dim3 grid = f16v_grid(a.g, lt4, a.g.nz);
-      if (odd) k_aa_f16v<true, true><<<grid, 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
+      static int blkl = -1;
+      if (blkl < 0) {
+        const char* e = getenv("BGK_AA_BLK");
+        blkl = e ? atoi(e) : 0;
+      }
+      if (odd && blkl) k_aa_f16v<true, true, true><<<grid, 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
+      else if (odd) k_aa_f16v<true, true><<<grid, 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
       else k_aa_f16v<false, true><<<grid, 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
     } else if (odd) {
       k_aa<F, true, true><<<sh.grid, sh.block, 0, st>>>(pops_of<S>(a), a.g, K);
@@ -1076,7 +1167,13 @@ static cudaError_t aa_impl(const Lattice& a, int odd, const StepK& K, int varian
   // FP16: four cells per thread where the box fits it (automatic or 4)
   if (lt4 >= 0) {
     const dim3 grid = f16v_grid(a.g, lt4, a.g.nz);
-    if (odd) k_aa_f16v<true, false><<<grid, 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
+    static int blk = -1;
+    if (blk < 0) {
+      const char* e = getenv("BGK_AA_BLK");
+      blk = e ? atoi(e) : 0;
+    }
+    if (odd && blk) k_aa_f16v<true, false, true><<<grid, 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
+    else if (odd) k_aa_f16v<true, false><<<grid, 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
     else k_aa_f16v<false, false><<<grid, 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
     return cudaGetLastError();
   }

@@ -816,7 +816,7 @@ __global__ void k_faith_snapshot(Pops<const S> a, Geo g, S* out) {
   }
 }
 
-template <class F, int LAY>
+template <class F, int LAY, bool FAITH = false>
 __global__ void __launch_bounds__(DIAG_THREADS) k_diag(Pops<const typename F::S> a, Geo g, double svisc,
                                                        double omega, typename F::R inv, double* partials,
                                                        typename F::R* vel, Halo<typename F::S> h,
@@ -853,7 +853,7 @@ __global__ void __launch_bounds__(DIAG_THREADS) k_diag(Pops<const typename F::S>
       if (LAY == LAY_TWO && h.in_lo[0] && (lo || hi)) {
         const int po = wrapi(i - cxq(q), g.nx) + g.sx * wrapi(j - cyq(q), g.ny);
         x[q] = N::wrap(F::dec(lo ? h.in_lo[zslot(q)][po] : h.in_hi[zslot(q)][po], inv));
-      } else if (LAY == LAY_TWO && (faith || faith_zero) &&
+      } else if (FAITH && LAY == LAY_TWO &&
                  (si < 0 || si >= g.nx || sj < 0 || sj >= g.ny || sk < 0 || sk >= g.nz)) {
         // faithful mode: the reference's ghost cell of this pull, filled two
         // steps earlier (or never)
@@ -1295,9 +1295,13 @@ template <class F, int LAY>
 static void diag_lay(const Lattice& a, double svisc, double omega, double scale, double* partials, void* vel,
                      const SlabLinks* halo, const void* faith, bool fzero, cudaStream_t st) {
   using S = typename F::S; using R = typename F::R;
-  k_diag<F, LAY><<<DIAG_BLOCKS, DIAG_THREADS, 0, st>>>(pops_of<const S>(a), a.g, svisc, omega, (R)(1.0 / scale),
-                                                       partials, (R*)vel, halo_of<S>(halo), (const S*)faith,
-                                                       fzero ? 1 : 0);
+  if (faith || fzero)
+    k_diag<F, LAY, true><<<DIAG_BLOCKS, DIAG_THREADS, 0, st>>>(pops_of<const S>(a), a.g, svisc, omega,
+                                                             (R)(1.0 / scale), partials, (R*)vel, halo_of<S>(halo),
+                                                             (const S*)faith, fzero ? 1 : 0);
+  else
+    k_diag<F, LAY><<<DIAG_BLOCKS, DIAG_THREADS, 0, st>>>(pops_of<const S>(a), a.g, svisc, omega, (R)(1.0 / scale),
+                                                         partials, (R*)vel, halo_of<S>(halo), nullptr, 0);
 }
 template <class F>
 static cudaError_t diag_impl(const Lattice& a, int lay, double svisc, double omega, double scale, double* partials,

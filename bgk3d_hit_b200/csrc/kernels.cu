@@ -11,8 +11,6 @@
 //                per-block partials
 //   k_enstrophy  0.5|curl u|^2 from the local velocity field
 //   k_shift3     shift-only stencil of SRC/do_somethingGPU.F90:37-100
-#include <cstdlib>
-
 #include "kernels.h"
 #include "reduce.cuh"
 
@@ -191,38 +189,6 @@ __device__ __forceinline__ void shift_rows(uint2 (&Y)[Q], const unsigned short (
   }
 }
 
-// Stores four cells' values Y (cells i0..i0+3) at elements i0 + cx ...
-// i0 + 3 + cx of row p: an aligned 8-byte store of the chunk at i0, completed
-// with the neighbouring lane's crossing value; edge lanes store their part of
-// the chunk and their crossing value with 4- and 2-byte stores.
-__device__ __forceinline__ void shift_out(uint2 Y, int cx, __half* p, int i0, int i_prev, int i_next,
-                                          const XLanes& xl) {
-  unsigned short* u = reinterpret_cast<unsigned short*>(p);
-  if (cx == 0) {
-    *reinterpret_cast<uint2*>(p + i0) = Y;
-  } else if (cx > 0) {  // cell i0+m -> element i0+m+1
-    const unsigned prev = __shfl_sync(0xffffffffu, Y.y >> 16, xl.src_prev);  // cell i0-1 of the lane before
-    const unsigned lo = __byte_perm(prev, Y.x, 0x5410), hi = __byte_perm(Y.x, Y.y, 0x5432);
-    if (!xl.edge_prev) {
-      *reinterpret_cast<uint2*>(p + i0) = make_uint2(lo, hi);
-    } else {
-      u[i0 + 1] = (unsigned short)(Y.x & 0xffffu);
-      *reinterpret_cast<unsigned*>(p + i0 + 2) = hi;
-    }
-    if (xl.edge_next) u[i_next] = (unsigned short)(Y.y >> 16);
-  } else {  // cell i0+m -> element i0+m-1
-    const unsigned next = __shfl_sync(0xffffffffu, Y.x & 0xffffu, xl.src_next);  // cell i0+4 of the lane after
-    const unsigned lo = __byte_perm(Y.x, Y.y, 0x5432), hi = __byte_perm(Y.y, next, 0x5432);
-    if (!xl.edge_next) {
-      *reinterpret_cast<uint2*>(p + i0) = make_uint2(lo, hi);
-    } else {
-      *reinterpret_cast<unsigned*>(p + i0) = lo;
-      u[i0 + 2] = (unsigned short)(Y.y >> 16);
-    }
-    if (xl.edge_prev) u[i_prev] = (unsigned short)(Y.x & 0xffffu);
-  }
-}
-
 template <bool LES>
 __global__ void __launch_bounds__(128, 5) k_two_f16v(Pops<const __half> src, Pops<__half> dst, Geo g, StepK K,
                                                   int log_tpr, int k0) {
@@ -381,11 +347,17 @@ __global__ void __launch_bounds__(256, 5) k_aa_f16_odd(Pops<__half> a, Geo g, St
 // and collision as k_two_f16v). Even step: slot q at x -> slot opp(q) at x,
 // 8-byte accesses, no exchange. Odd step: slot opp(q) at x - c_q -> slot q at
 // x + c_q, with the x-crossing values moved between lanes on both the load and
-// the store side. Every (location, slot) pair is still read and written by the
+// the store side; on the store side a warp-edge lane gets its crossing value
+// from the neighbouring warp of the block through shared memory after a block
+// barrier, so only block boundaries need partial stores (a warp edge with 2-
+// and 4-byte stores costs about as much as the rest of the warp's stores of
+// that population: 240 -> 223 us per 256^3 odd step, AA pair 77.1 -> 80.1
+// GLUPS). Every (location, slot) pair is still read and written by the
 // thread of the cell that owns it in the one-cell-per-thread kernel, or by a
 // lane of the same warp after a shuffle that orders it behind the owner's
-// loads, so the in-place update stays race-free. 128-thread blocks at 96
-// registers (5 blocks per SM) like k_two_f16v. The odd step stores to the
+// loads, or by a lane of another warp of the block after the barrier that
+// follows every warp's loads, so the in-place update stays race-free.
+// 128-thread blocks at 96 registers (5 blocks per SM) like k_two_f16v. The odd step stores to the
 // rows it loaded from; left alone, the compiler keeps those 18 row addresses
 // live through the collision, so the BGK odd step recomputes them from an
 // opaque copy of (j, k) and fits 96 registers without spills (5 blocks per
@@ -396,13 +368,16 @@ __global__ void __launch_bounds__(256, 5) k_aa_f16_odd(Pops<__half> a, Geo g, St
 // thread; with the loads issued before the shuffles and the even step at 96
 // registers as well, 76.9. The LES odd step recomputes its store rows the
 // same way (96 registers, a few spilled bytes).
-// Store side of the odd step when the x-crossing values of warp edges come
-// from the neighbouring warp of the same block through shared memory: an edge
-// lane whose neighbour warp is in the block stores a whole aligned 8-byte
-// chunk (the crossing element included) and the neighbour skips its 2-byte
-// store of that element; edges at block boundaries keep the partial stores
-// of shift_out. from_prev / from_next: the neighbour warp's crossing value.
-__device__ __forceinline__ void shift_out_blk(uint2 Y, int cx, __half* p, int i0, int i_prev, int i_next,
+// Store side of the AA odd step: stores four cells' values Y (cells
+// i0..i0+3) at elements i0 + cx ... i0 + 3 + cx of row p as one aligned
+// 8-byte chunk, completed with the neighbouring lane's crossing value (warp
+// shuffle). A warp-edge lane takes that value from the neighbouring warp
+// through shared memory (from_prev / from_next) when that warp is in the same
+// block (prev_in / next_in) and stores its whole chunk, the neighbour then
+// skipping its store of the crossing element; at block boundaries the edge
+// lanes store their part of the chunk and their crossing value with 4- and
+// 2-byte stores.
+__device__ __forceinline__ void shift_out(uint2 Y, int cx, __half* p, int i0, int i_prev, int i_next,
                                               const XLanes& xl, bool prev_in, bool next_in, unsigned from_prev,
                                               unsigned from_next) {
   unsigned short* u = reinterpret_cast<unsigned short*>(p);
@@ -433,15 +408,15 @@ __device__ __forceinline__ void shift_out_blk(uint2 Y, int cx, __half* p, int i0
   }
 }
 
-template <bool ODD, bool LES, bool BLK = false>
+template <bool ODD, bool LES>
 __global__ void __launch_bounds__(128, 5) k_aa_f16v(Pops<__half> a, Geo g, StepK K, int log_tpr) {
   const int tpr = 1 << log_tpr;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int j0 = t >> log_tpr, pos = t & (tpr - 1);
   const int k = blockIdx.y;
   const bool valid = j0 < g.ny;  // whole warps: ny*tpr is a multiple of 32
-  if (!(ODD && BLK) && !valid) return;
-  const int j = valid ? j0 : 0;  // an idle warp of the block-edge variant only reaches its barrier
+  if (!ODD && !valid) return;
+  const int j = valid ? j0 : 0;  // an idle warp of the odd step only reaches its barrier
   const XLanes xl(tpr, pos, threadIdx.x & 31);
   const int i0 = pos * 4;
   const int jm = j == 0 ? g.ny - 1 : j - 1, jp = j == g.ny - 1 ? 0 : j + 1;
@@ -454,7 +429,7 @@ __global__ void __launch_bounds__(128, 5) k_aa_f16v(Pops<__half> a, Geo g, StepK
     return g.sx * (jj + g.ny * kk);
   };
   uint2 Y[Q];
-  if (ODD && BLK && !valid) {
+  if (ODD && !valid) {
 #pragma unroll
     for (int q = 0; q < Q; ++q) Y[q] = make_uint2(0u, 0u);
   } else if (ODD) {
@@ -472,15 +447,15 @@ __global__ void __launch_bounds__(128, 5) k_aa_f16v(Pops<__half> a, Geo g, StepK
 #pragma unroll
     for (int q = 0; q < Q; ++q) Y[q] = __ldg(reinterpret_cast<const uint2*>(a.p[q] + row(0, 0) + i0));
   }
-  if (!(ODD && BLK && !valid)) collide4_f16<LES>(Y, K);
-  // block-edge variant: the warps' crossing values (cx > 0 populations: the
-  // last lane's last cell; cx < 0: the first lane's first cell) through
-  // shared memory; the barrier also orders every warp's loads before any
-  // warp's stores of its neighbours' crossing elements
-  __shared__ unsigned xs_last[ODD && BLK ? 4 : 1][5], xs_first[ODD && BLK ? 4 : 1][5];
+  if (valid) collide4_f16<LES>(Y, K);
+  // odd step: the warps' crossing values (cx > 0 populations: the last
+  // lane's last cell; cx < 0: the first lane's first cell) through shared
+  // memory; the barrier also orders every warp's loads before any warp's
+  // stores of its neighbours' crossing elements
+  __shared__ unsigned xs_last[ODD ? 4 : 1][5], xs_first[ODD ? 4 : 1][5];
   bool prev_in = false, next_in = false;
   int wprev = 0, wnext = 0;
-  if (ODD && BLK) {
+  if (ODD) {
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (tpr >= 32) {
       const int nw = tpr >> 5, r = pos >> 5;  // warps per row, this warp's place in its row
@@ -519,13 +494,10 @@ __global__ void __launch_bounds__(128, 5) k_aa_f16v(Pops<__half> a, Geo g, StepK
   for (int q = 0; q < Q; ++q) {
     if (!ODD) {
       *reinterpret_cast<uint2*>(a.p[oppq(q)] + row(0, 0) + i0) = Y[q];
-    } else if (BLK) {
+    } else {
       const unsigned fp = cxq(q) > 0 && xl.edge_prev && prev_in ? xs_last[wprev][q] : 0u;
       const unsigned fn = cxq(q) < 0 && xl.edge_next && next_in ? xs_first[wnext][q - 9] : 0u;
-      shift_out_blk(Y[q], cxq(q), a.p[q] + row_out(cyq(q), czq(q)), i0, i_prev, i_next, xl, prev_in, next_in, fp,
-                    fn);
-    } else {
-      shift_out(Y[q], cxq(q), a.p[q] + row_out(cyq(q), czq(q)), i0, i_prev, i_next, xl);
+      shift_out(Y[q], cxq(q), a.p[q] + row_out(cyq(q), czq(q)), i0, i_prev, i_next, xl, prev_in, next_in, fp, fn);
     }
   }
 }
@@ -1144,13 +1116,7 @@ static cudaError_t aa_impl(const Lattice& a, int odd, const StepK& K, int varian
   if (K.les) {
     if (lt4 >= 0) {
       const dim3 grid = f16v_grid(a.g, lt4, a.g.nz);
-      static int blkl = -1;
-      if (blkl < 0) {
-        const char* e = getenv("BGK_AA_BLK");
-        blkl = e ? atoi(e) : 0;
-      }
-      if (odd && blkl) k_aa_f16v<true, true, true><<<grid, 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
-      else if (odd) k_aa_f16v<true, true><<<grid, 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
+      if (odd) k_aa_f16v<true, true><<<grid, 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
       else k_aa_f16v<false, true><<<grid, 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
     } else if (odd) {
       k_aa<F, true, true><<<sh.grid, sh.block, 0, st>>>(pops_of<S>(a), a.g, K);
@@ -1167,13 +1133,7 @@ static cudaError_t aa_impl(const Lattice& a, int odd, const StepK& K, int varian
   // FP16: four cells per thread where the box fits it (automatic or 4)
   if (lt4 >= 0) {
     const dim3 grid = f16v_grid(a.g, lt4, a.g.nz);
-    static int blk = -1;
-    if (blk < 0) {
-      const char* e = getenv("BGK_AA_BLK");
-      blk = e ? atoi(e) : 0;
-    }
-    if (odd && blk) k_aa_f16v<true, false, true><<<grid, 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
-    else if (odd) k_aa_f16v<true, false><<<grid, 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
+    if (odd) k_aa_f16v<true, false><<<grid, 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
     else k_aa_f16v<false, false><<<grid, 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
     return cudaGetLastError();
   }

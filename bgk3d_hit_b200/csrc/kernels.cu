@@ -11,8 +11,6 @@
 //                per-block partials
 //   k_enstrophy  0.5|curl u|^2 from the local velocity field
 //   k_shift3     shift-only stencil of SRC/do_somethingGPU.F90:37-100
-#include <cstdlib>
-
 #include "kernels.h"
 #include "reduce.cuh"
 
@@ -191,68 +189,15 @@ __device__ __forceinline__ void shift_rows(uint2 (&Y)[Q], const unsigned short (
   }
 }
 
-// The warps of a 128-thread block that hold the x-neighbours of a warp's
-// first and last cells, for rows of tpr >= 32 threads: a row of up to four
-// warps lies in one block (and wraps around within it); longer rows cross
-// block boundaries, where prev_in / next_in are false.
-struct WarpNb {
-  bool prev_in = false, next_in = false;
-  int wprev = 0, wnext = 0;
-};
-__device__ __forceinline__ WarpNb warp_neighbours(int tpr, int pos) {
-  WarpNb n;
-  if (tpr < 32) return n;
-  const int w = threadIdx.x >> 5, nw = tpr >> 5, r = pos >> 5;  // warps per row, this warp's place in its row
-  if (nw <= 4) {
-    n.prev_in = n.next_in = true;
-    n.wprev = w - r + (r + nw - 1) % nw;
-    n.wnext = w - r + (r + 1) % nw;
-  } else {
-    n.prev_in = w > 0;
-    n.next_in = w < 3;
-    n.wprev = w - 1;
-    n.wnext = w + 1;
-  }
-  return n;
-}
-
-// Load side of the x-shifted rows with block-local warp edges: the crossing
-// elements of the warp-edge lanes come from the neighbouring warp's chunks
-// through shared memory (after a block barrier) instead of 2-byte loads,
-// where that warp is in the block. Y: the aligned chunks just loaded; E: the
-// crossing elements loaded by edge lanes whose neighbour is outside the block.
-__device__ __forceinline__ void exchange_edges(const uint2 (&Y)[Q], unsigned short (&E)[Q], const XLanes& xl,
-                                               const WarpNb& nb, bool valid, unsigned (&last)[4][5],
-                                               unsigned (&first)[4][5]) {
-  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if (valid && lane == 31) {
-#pragma unroll
-    for (int q = 0; q < 5; ++q) last[w][q] = Y[q].y >> 16;  // element i0+3 of the cx > 0 rows
-  }
-  if (valid && lane == 0) {
-#pragma unroll
-    for (int q = 9; q < 14; ++q) first[w][q - 9] = Y[q].x & 0xffffu;  // element i0 of the cx < 0 rows
-  }
-  __syncthreads();
-#pragma unroll
-  for (int q = 0; q < Q; ++q) {
-    if (cxq(q) > 0 && xl.edge_prev && nb.prev_in) E[q] = (unsigned short)last[nb.wprev][q];
-    if (cxq(q) < 0 && xl.edge_next && nb.next_in) E[q] = (unsigned short)first[nb.wnext][q - 9];
-  }
-}
-
-template <bool LES, bool LX = false>
+template <bool LES>
 __global__ void __launch_bounds__(128, 5) k_two_f16v(Pops<const __half> src, Pops<__half> dst, Geo g, StepK K,
                                                   int log_tpr, int k0) {
   const int tpr = 1 << log_tpr;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j0 = t >> log_tpr, pos = t & (tpr - 1);
+  const int j = t >> log_tpr, pos = t & (tpr - 1);
   const int k = blockIdx.y + k0;  // planes k0 .. k0 + gridDim.y - 1
-  const bool valid = j0 < g.ny;  // whole warps: ny*tpr is a multiple of 32
-  if (!LX && !valid) return;
-  const int j = valid ? j0 : 0;  // an idle warp only reaches the barrier
+  if (j >= g.ny) return;  // whole warps: ny*tpr is a multiple of 32
   const XLanes xl(tpr, pos, threadIdx.x & 31);
-  const WarpNb nb = LX ? warp_neighbours(tpr, pos) : WarpNb{};
   const int i0 = pos * 4;
   const int jm = j == 0 ? g.ny - 1 : j - 1, jp = j == g.ny - 1 ? 0 : j + 1;
   const int km = k == 0 ? g.nz - 1 : k - 1, kp = k == g.nz - 1 ? 0 : k + 1;
@@ -265,17 +210,10 @@ __global__ void __launch_bounds__(128, 5) k_two_f16v(Pops<const __half> src, Pop
     const int jj = cyq(q) > 0 ? jm : (cyq(q) < 0 ? jp : j);
     const int kk = czq(q) > 0 ? km : (czq(q) < 0 ? kp : k);
     const __half* p = (q == Q - 1 ? (const __half*)dst.p[Q - 1] : src.p[q]) + g.sx * (jj + g.ny * kk);
-    Y[q] = make_uint2(0u, 0u);
-    E[q] = 0;
-    if (!valid) continue;
     Y[q] = (q == Q - 1) ? *reinterpret_cast<const uint2*>(p + i0) : __ldg(reinterpret_cast<const uint2*>(p + i0));
-    if (cxq(q) > 0 && xl.edge_prev && !nb.prev_in) E[q] = ldg_u16(p + i_prev);
-    if (cxq(q) < 0 && xl.edge_next && !nb.next_in) E[q] = ldg_u16(p + i_next);
-  }
-  if (LX) {
-    __shared__ unsigned xlast[4][5], xfirst[4][5];
-    exchange_edges(Y, E, xl, nb, valid, xlast, xfirst);
-    if (!valid) return;
+    E[q] = 0;
+    if (cxq(q) > 0 && xl.edge_prev) E[q] = ldg_u16(p + i_prev);
+    if (cxq(q) < 0 && xl.edge_next) E[q] = ldg_u16(p + i_next);
   }
   shift_rows(Y, E, xl);
   collide4_f16<LES>(Y, K);
@@ -470,7 +408,7 @@ __device__ __forceinline__ void shift_out(uint2 Y, int cx, __half* p, int i0, in
   }
 }
 
-template <bool ODD, bool LES, bool LX = false>
+template <bool ODD, bool LES>
 __global__ void __launch_bounds__(128, 5) k_aa_f16v(Pops<__half> a, Geo g, StepK K, int log_tpr) {
   const int tpr = 1 << log_tpr;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -491,26 +429,20 @@ __global__ void __launch_bounds__(128, 5) k_aa_f16v(Pops<__half> a, Geo g, StepK
     return g.sx * (jj + g.ny * kk);
   };
   uint2 Y[Q];
-  if (ODD) {
-    // every thread of the block reaches the barriers below; idle warps
-    // (rows beyond ny) load and store nothing
-    const WarpNb nbl = LX ? warp_neighbours(tpr, pos) : WarpNb{};
+  if (ODD && !valid) {
+#pragma unroll
+    for (int q = 0; q < Q; ++q) Y[q] = make_uint2(0u, 0u);
+  } else if (ODD) {
     unsigned short E[Q];
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
-      Y[q] = make_uint2(0u, 0u);
-      E[q] = 0;
-      if (!valid) continue;
       const __half* p = a.p[oppq(q)] + row(-cyq(q), -czq(q));
       Y[q] = __ldg(reinterpret_cast<const uint2*>(p + i0));
-      if (cxq(q) > 0 && xl.edge_prev && !nbl.prev_in) E[q] = ldg_u16(p + i_prev);
-      if (cxq(q) < 0 && xl.edge_next && !nbl.next_in) E[q] = ldg_u16(p + i_next);
+      E[q] = 0;
+      if (cxq(q) > 0 && xl.edge_prev) E[q] = ldg_u16(p + i_prev);
+      if (cxq(q) < 0 && xl.edge_next) E[q] = ldg_u16(p + i_next);
     }
-    if (LX) {
-      __shared__ unsigned ylast[4][5], yfirst[4][5];
-      exchange_edges(Y, E, xl, nbl, valid, ylast, yfirst);
-    }
-    if (valid) shift_rows(Y, E, xl);
+    shift_rows(Y, E, xl);
   } else {
 #pragma unroll
     for (int q = 0; q < Q; ++q) Y[q] = __ldg(reinterpret_cast<const uint2*>(a.p[q] + row(0, 0) + i0));
@@ -1096,15 +1028,6 @@ static dim3 f16v_grid(const Geo& g, int log_tpr, int planes) {
 }
 
 // log2(nx/V) when the V-cells-per-thread FP16 kernel applies, else -1.
-static bool f16_lx() {
-  static int v = -1;
-  if (v < 0) {
-    const char* e = getenv("BGK_F16_LX");
-    v = e ? atoi(e) : 0;
-  }
-  return v != 0;
-}
-
 static int f16v_log_tpr(const Geo& g, int V) {
   if (g.nx % V) return -1;
   const int tpr = g.nx / V;
@@ -1128,7 +1051,7 @@ static cudaError_t two_impl(const Lattice& s, const Lattice& d, const StepK& K, 
       Pops<__half> ph = pops_of<__half>(d);
       ph.p[Q - 1] = (__half*)s.p[Q - 1];
       const dim3 grid = f16v_grid(s.g, lt, s.g.nz);
-      { if (f16_lx()) k_two_f16v<true, true><<<grid, 128, 0, st>>>(pops_of<const __half>(s), ph, s.g, K, lt, 0); else k_two_f16v<true><<<grid, 128, 0, st>>>(pops_of<const __half>(s), ph, s.g, K, lt, 0); }
+      k_two_f16v<true><<<grid, 128, 0, st>>>(pops_of<const __half>(s), ph, s.g, K, lt, 0);
     } else {
       k_two<F, true><<<sh.grid, sh.block, 0, st>>>(ps, pd, s.g, K);
     }
@@ -1151,8 +1074,7 @@ static cudaError_t two_impl(const Lattice& s, const Lattice& d, const StepK& K, 
       dim3 grid((unsigned)((threads + (V == 4 ? 127 : 255)) / (V == 4 ? 128 : 256)), s.g.nz);
       Pops<__half> ph = pops_of<__half>(d);
       ph.p[Q - 1] = (__half*)s.p[Q - 1];
-      if (V == 4 && f16_lx()) k_two_f16v<false, true><<<grid, 128, 0, st>>>(pops_of<const __half>(s), ph, s.g, K, lt, 0);
-      else if (V == 4) k_two_f16v<false><<<grid, 128, 0, st>>>(pops_of<const __half>(s), ph, s.g, K, lt, 0);
+      if (V == 4) k_two_f16v<false><<<grid, 128, 0, st>>>(pops_of<const __half>(s), ph, s.g, K, lt, 0);
       else k_two_f16v2<<<grid, 256, 0, st>>>(pops_of<const __half>(s), ph, s.g, K, lt);
       return cudaGetLastError();
     }
@@ -1194,8 +1116,7 @@ static cudaError_t aa_impl(const Lattice& a, int odd, const StepK& K, int varian
   if (K.les) {
     if (lt4 >= 0) {
       const dim3 grid = f16v_grid(a.g, lt4, a.g.nz);
-      if (odd && f16_lx()) k_aa_f16v<true, true, true><<<grid, 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
-      else if (odd) k_aa_f16v<true, true><<<grid, 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
+      if (odd) k_aa_f16v<true, true><<<grid, 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
       else k_aa_f16v<false, true><<<grid, 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
     } else if (odd) {
       k_aa<F, true, true><<<sh.grid, sh.block, 0, st>>>(pops_of<S>(a), a.g, K);
@@ -1212,8 +1133,7 @@ static cudaError_t aa_impl(const Lattice& a, int odd, const StepK& K, int varian
   // FP16: four cells per thread where the box fits it (automatic or 4)
   if (lt4 >= 0) {
     const dim3 grid = f16v_grid(a.g, lt4, a.g.nz);
-    if (odd && f16_lx()) k_aa_f16v<true, false, true><<<grid, 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
-    else if (odd) k_aa_f16v<true, false><<<grid, 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
+    if (odd) k_aa_f16v<true, false><<<grid, 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
     else k_aa_f16v<false, false><<<grid, 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
     return cudaGetLastError();
   }

@@ -11,8 +11,6 @@
 //                per-block partials
 //   k_enstrophy  0.5|curl u|^2 from the local velocity field
 //   k_shift3     shift-only stencil of SRC/do_somethingGPU.F90:37-100
-#include <cstdlib>
-
 #include "kernels.h"
 #include "reduce.cuh"
 
@@ -336,64 +334,6 @@ __device__ __forceinline__ void aa_cell(Pops<typename F::S>& a, const Geo& g, co
 template <class F, bool ODD, bool LES = false>
 __global__ void __launch_bounds__(256) k_aa(Pops<typename F::S> a, Geo g, StepK K) {
   aa_cell<F, ODD, LES>(a, g, K);
-}
-
-// AA odd step, one cell per thread, with the x-shifted stores staged in
-// shared memory: the outputs of the ten populations with c_x != 0 go to a
-// block row buffer at their shifted place; after a block barrier (which also
-// orders every thread's loads before the stores) each thread stores the
-// element at its own x, so each warp writes whole aligned segments. The
-// element that leaves the block (at a block boundary of a row longer than
-// the block) is stored by its own cell's thread, as in k_aa. Requires the
-// launch shape of cell_shape with 128 x 2 blocks and nx a multiple of 128.
-template <class F, bool LES>
-__global__ void __launch_bounds__(256) k_aa_odd_blk(Pops<typename F::S> a, Geo g, StepK K) {
-  using S = typename F::S;
-  __shared__ S xs[2][10][130];  // [threadIdx.y][population with c_x != 0][1 + x + c_x]
-  const int bx = blockDim.x, tx = threadIdx.x, ty = threadIdx.y;
-  const int ib = blockIdx.x * bx, i = ib + tx;
-  const int j0 = blockIdx.y * blockDim.y + ty;
-  const int k = blockIdx.z;
-  const bool valid = j0 < g.ny;  // i < nx: nx is a multiple of blockDim.x
-  const int j = valid ? j0 : 0;
-  const int im = i == 0 ? g.nx - 1 : i - 1, ip = i == g.nx - 1 ? 0 : i + 1;
-  const int jm = j == 0 ? g.ny - 1 : j - 1, jp = j == g.ny - 1 ? 0 : j + 1;
-  const int km = k == 0 ? g.nz - 1 : k - 1, kp = k == g.nz - 1 ? 0 : k + 1;
-  auto back = [&](int q) {  // x - c_q
-    const int ii = cxq(q) > 0 ? im : (cxq(q) < 0 ? ip : i);
-    const int jj = cyq(q) > 0 ? jm : (cyq(q) < 0 ? jp : j);
-    const int kk = czq(q) > 0 ? km : (czq(q) < 0 ? kp : k);
-    return ii + g.sx * (jj + g.ny * kk);
-  };
-  S v[Q];
-  if (valid) {
-#pragma unroll
-    for (int q = 0; q < Q; ++q) v[q] = ldg(a.p[oppq(q)] + back(q));
-    F::template cell<LES>(v, K);
-#pragma unroll
-    for (int q = 0; q < Q; ++q)
-      if (cxq(q) != 0) xs[ty][q < 5 ? q : q - 4][1 + tx + cxq(q)] = v[q];
-  }
-  __syncthreads();
-  if (!valid) return;
-  const bool whole_row = bx == g.nx;
-#pragma unroll
-  for (int q = 0; q < Q; ++q) {
-    const int cx = cxq(q);
-    if (cx == 0) {
-      a.p[q][back(oppq(q))] = v[q];  // slot q at x + c_q
-      continue;
-    }
-    const int jj = cyq(q) > 0 ? jp : (cyq(q) < 0 ? jm : j);
-    const int kk = czq(q) > 0 ? kp : (czq(q) < 0 ? km : k);
-    S* row = a.p[q] + g.sx * (jj + g.ny * kk);
-    const int e = q < 5 ? q : q - 4;
-    int src = tx - cx;  // block-local cell whose value lands at this x
-    if (whole_row) src = src < 0 ? src + bx : (src >= bx ? src - bx : src);
-    if (src >= 0 && src < bx) row[i] = xs[ty][e][1 + src + cx];
-    // this cell's value leaves the block: store it here
-    if (!whole_row && ((cx > 0 && tx == bx - 1) || (cx < 0 && tx == 0))) row[cx > 0 ? ip : im] = v[q];
-  }
 }
 
 // The FP16 odd step (BGK) is latency-bound on registers: capped at 48 (5
@@ -1197,15 +1137,8 @@ static cudaError_t aa_impl(const Lattice& a, int odd, const StepK& K, int varian
     else k_aa_f16v<false, false><<<grid, 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
     return cudaGetLastError();
   }
-  static int blk = -1;
-  if (blk < 0) {
-    const char* e = getenv("BGK_AA1_BLK");
-    blk = e ? atoi(e) : 0;
-  }
-  const bool fits_blk = sh.block.x == 128 && sh.block.y == 2 && a.g.nx % 128 == 0;  // xs holds 2 rows of 128
   if (odd && F::id == FORM_F16)
     k_aa_f16_odd<<<sh.grid, sh.block, 0, st>>>(pops_of<__half>(a), a.g, K);
-  else if (odd && blk && fits_blk) k_aa_odd_blk<F, false><<<sh.grid, sh.block, 0, st>>>(pops_of<S>(a), a.g, K);
   else if (odd) k_aa<F, true><<<sh.grid, sh.block, 0, st>>>(pops_of<S>(a), a.g, K);
   else k_aa<F, false><<<sh.grid, sh.block, 0, st>>>(pops_of<S>(a), a.g, K);
   return cudaGetLastError();

@@ -222,6 +222,72 @@ __global__ void __launch_bounds__(128, 5) k_two_f16v(Pops<const __half> src, Pop
   for (int q = 0; q < Q; ++q) *reinterpret_cast<uint2*>(dst.p[q] + o) = Y[q];
 }
 
+// FP32 two-lattice step with 2 cells per thread and 8-byte accesses (tpr =
+// nx/2 threads per row): k_two_f16v's row split and x-crossing shuffles on
+// chunks of two floats, F32::cell's arithmetic on each cell, so the results
+// are those of k_two<F32>.
+// x-shifted rows of two-float chunks: shift_rows on FP32 pairs.
+__device__ __forceinline__ void shift_rows_f32(float2 (&Y)[Q], const float (&E)[Q], const XLanes& xl) {
+#pragma unroll
+  for (int q = 0; q < Q; ++q) {
+    const float2 A = Y[q];
+    if (cxq(q) > 0) {  // elements i0-1, i0
+      float prev = __shfl_sync(0xffffffffu, A.y, xl.src_prev);
+      if (xl.edge_prev) prev = E[q];
+      Y[q] = make_float2(prev, A.x);
+    } else if (cxq(q) < 0) {  // elements i0+1, i0+2
+      float next = __shfl_sync(0xffffffffu, A.x, xl.src_next);
+      if (xl.edge_next) next = E[q];
+      Y[q] = make_float2(A.y, next);
+    }
+  }
+}
+
+template <bool LES>
+__global__ void __launch_bounds__(128, 5) k_two_f32v(Pops<const float> src, Pops<float> dst, Geo g, StepK K,
+                                                  int log_tpr, int k0) {
+  const int tpr = 1 << log_tpr;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = t >> log_tpr, pos = t & (tpr - 1);
+  const int k = blockIdx.y + k0;  // planes k0 .. k0 + gridDim.y - 1
+  if (j >= g.ny) return;  // whole warps: ny*tpr is a multiple of 32
+  const XLanes xl(tpr, pos, threadIdx.x & 31);
+  const int i0 = pos * 2;
+  const int jm = j == 0 ? g.ny - 1 : j - 1, jp = j == g.ny - 1 ? 0 : j + 1;
+  const int km = k == 0 ? g.nz - 1 : k - 1, kp = k == g.nz - 1 ? 0 : k + 1;
+  const int i_prev = pos == 0 ? g.nx - 1 : i0 - 1;
+  const int i_next = pos == tpr - 1 ? 0 : i0 + 2;
+  float2 Y[Q];  // two cells' values per population, cell m in component m
+  float E[Q];
+#pragma unroll
+  for (int q = 0; q < Q; ++q) {
+    const int jj = cyq(q) > 0 ? jm : (cyq(q) < 0 ? jp : j);
+    const int kk = czq(q) > 0 ? km : (czq(q) < 0 ? kp : k);
+    // pop 19 in place (src.p[18] == dst.p[18]) with a plain load
+    const float* p = (q == Q - 1 ? (const float*)dst.p[Q - 1] : src.p[q]) + g.sx * (jj + g.ny * kk);
+    Y[q] = (q == Q - 1) ? *reinterpret_cast<const float2*>(p + i0) : __ldg(reinterpret_cast<const float2*>(p + i0));
+    E[q] = 0.f;
+    if (cxq(q) > 0 && xl.edge_prev) E[q] = __ldg(p + i_prev);
+    if (cxq(q) < 0 && xl.edge_next) E[q] = __ldg(p + i_next);
+  }
+  shift_rows_f32(Y, E, xl);
+#pragma unroll
+  for (int m = 0; m < 2; ++m) {
+    float s[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) s[q] = m ? Y[q].y : Y[q].x;
+    F32::cell<LES>(s, K);
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      if (m) Y[q].y = s[q];
+      else Y[q].x = s[q];
+    }
+  }
+  const int o = i0 + g.sx * (j + g.ny * k);
+#pragma unroll
+  for (int q = 0; q < Q; ++q) *reinterpret_cast<float2*>(dst.p[q] + o) = Y[q];
+}
+
 // Same with 2 cells per thread and 4-byte accesses (tpr = nx/2 threads per row).
 __global__ void __launch_bounds__(256, 4) k_two_f16v2(Pops<const __half> src, Pops<__half> dst, Geo g, StepK K,
                                                    int log_tpr) {
@@ -498,6 +564,138 @@ __global__ void __launch_bounds__(128, 5) k_aa_f16v(Pops<__half> a, Geo g, StepK
       const unsigned fp = cxq(q) > 0 && xl.edge_prev && prev_in ? xs_last[wprev][q] : 0u;
       const unsigned fn = cxq(q) < 0 && xl.edge_next && next_in ? xs_first[wnext][q - 9] : 0u;
       shift_out(Y[q], cxq(q), a.p[q] + row_out(cyq(q), czq(q)), i0, i_prev, i_next, xl, prev_in, next_in, fp, fn);
+    }
+  }
+}
+
+// FP32 AA pattern with two cells per thread: k_aa_f16v's row split (tpr =
+// nx/2 threads per row), x-crossing shuffles and block-local warp-edge stores
+// on 8-byte chunks of two floats, F32::cell's arithmetic (the reference's
+// order) on each cell, so the results are those of k_aa<F32, ODD>. The same
+// ownership argument keeps the in-place update race-free.
+// Store side of the FP32 odd step: cells i0, i0+1 go to elements i0 + cx,
+// i0 + 1 + cx of row p, stored as the aligned chunk (i0, i0+1) completed with
+// the neighbouring lane's crossing value, as shift_out does for FP16.
+__device__ __forceinline__ void shift_out_f32(float2 Y, int cx, float* p, int i0, int i_prev, int i_next,
+                                              const XLanes& xl, bool prev_in, bool next_in, float from_prev,
+                                              float from_next) {
+  if (cx == 0) {
+    *reinterpret_cast<float2*>(p + i0) = Y;
+  } else if (cx > 0) {  // cell i0+m -> element i0+m+1
+    float prev = __shfl_sync(0xffffffffu, Y.y, xl.src_prev);  // cell i0-1 of the lane before
+    if (xl.edge_prev && prev_in) prev = from_prev;
+    if (!xl.edge_prev || prev_in) *reinterpret_cast<float2*>(p + i0) = make_float2(prev, Y.x);
+    else p[i0 + 1] = Y.x;
+    if (xl.edge_next && !next_in) p[i_next] = Y.y;
+  } else {  // cell i0+m -> element i0+m-1
+    float next = __shfl_sync(0xffffffffu, Y.x, xl.src_next);  // cell i0+2 of the lane after
+    if (xl.edge_next && next_in) next = from_next;
+    if (!xl.edge_next || next_in) *reinterpret_cast<float2*>(p + i0) = make_float2(Y.y, next);
+    else p[i0] = Y.y;
+    if (xl.edge_prev && !prev_in) p[i_prev] = Y.x;
+  }
+}
+
+template <bool ODD, bool LES>
+__global__ void __launch_bounds__(128, 5) k_aa_f32v(Pops<float> a, Geo g, StepK K, int log_tpr) {
+  const int tpr = 1 << log_tpr;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j0 = t >> log_tpr, pos = t & (tpr - 1);
+  const int k = blockIdx.y;
+  const bool valid = j0 < g.ny;  // whole warps: ny*tpr is a multiple of 32
+  if (!ODD && !valid) return;
+  const int j = valid ? j0 : 0;  // an idle warp of the odd step only reaches its barrier
+  const XLanes xl(tpr, pos, threadIdx.x & 31);
+  const int i0 = pos * 2;
+  const int jm = j == 0 ? g.ny - 1 : j - 1, jp = j == g.ny - 1 ? 0 : j + 1;
+  const int km = k == 0 ? g.nz - 1 : k - 1, kp = k == g.nz - 1 ? 0 : k + 1;
+  const int i_prev = pos == 0 ? g.nx - 1 : i0 - 1;
+  const int i_next = pos == tpr - 1 ? 0 : i0 + 2;
+  auto row = [&](int dy, int dz) {  // row offset of (j + dy, k + dz), dy, dz in {-1, 0, 1}
+    const int jj = dy > 0 ? jp : (dy < 0 ? jm : j);
+    const int kk = dz > 0 ? kp : (dz < 0 ? km : k);
+    return g.sx * (jj + g.ny * kk);
+  };
+  float2 Y[Q];
+  if (ODD && !valid) {
+#pragma unroll
+    for (int q = 0; q < Q; ++q) Y[q] = make_float2(0.f, 0.f);
+  } else if (ODD) {
+    float E[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      const float* p = a.p[oppq(q)] + row(-cyq(q), -czq(q));
+      Y[q] = __ldg(reinterpret_cast<const float2*>(p + i0));
+      E[q] = 0.f;
+      if (cxq(q) > 0 && xl.edge_prev) E[q] = __ldg(p + i_prev);
+      if (cxq(q) < 0 && xl.edge_next) E[q] = __ldg(p + i_next);
+    }
+    shift_rows_f32(Y, E, xl);
+  } else {
+#pragma unroll
+    for (int q = 0; q < Q; ++q) Y[q] = __ldg(reinterpret_cast<const float2*>(a.p[q] + row(0, 0) + i0));
+  }
+  if (valid) {
+#pragma unroll
+    for (int m = 0; m < 2; ++m) {
+      float s[Q];
+#pragma unroll
+      for (int q = 0; q < Q; ++q) s[q] = m ? Y[q].y : Y[q].x;
+      F32::cell<LES>(s, K);
+#pragma unroll
+      for (int q = 0; q < Q; ++q) {
+        if (m) Y[q].y = s[q];
+        else Y[q].x = s[q];
+      }
+    }
+  }
+  __shared__ float xs_last[ODD ? 4 : 1][5], xs_first[ODD ? 4 : 1][5];
+  bool prev_in = false, next_in = false;
+  int wprev = 0, wnext = 0;
+  if (ODD) {
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (tpr >= 32) {
+      const int nw = tpr >> 5, r = pos >> 5;  // warps per row, this warp's place in its row
+      if (nw <= 4) {  // the whole row in this block
+        prev_in = next_in = true;
+        wprev = w - r + (r + nw - 1) % nw;
+        wnext = w - r + (r + 1) % nw;
+      } else {
+        prev_in = w > 0;
+        next_in = w < 3;
+        wprev = w - 1;
+        wnext = w + 1;
+      }
+      if (valid && lane == 31) {
+#pragma unroll
+        for (int q = 0; q < 5; ++q) xs_last[w][q] = Y[q].y;
+      }
+      if (valid && lane == 0) {
+#pragma unroll
+        for (int q = 9; q < 14; ++q) xs_first[w][q - 9] = Y[q].x;
+      }
+    }
+    __syncthreads();
+    if (!valid) return;
+  }
+  int js = j, ks = k;  // store rows: recomputed after the collision
+  if (ODD) asm volatile("" : "+r"(js), "+r"(ks));
+  const int jms = js == 0 ? g.ny - 1 : js - 1, jps = js == g.ny - 1 ? 0 : js + 1;
+  const int kms = ks == 0 ? g.nz - 1 : ks - 1, kps = ks == g.nz - 1 ? 0 : ks + 1;
+  auto row_out = [&](int dy, int dz) {
+    const int jj = dy > 0 ? jps : (dy < 0 ? jms : js);
+    const int kk = dz > 0 ? kps : (dz < 0 ? kms : ks);
+    return g.sx * (jj + g.ny * kk);
+  };
+#pragma unroll
+  for (int q = 0; q < Q; ++q) {
+    if (!ODD) {
+      *reinterpret_cast<float2*>(a.p[oppq(q)] + row(0, 0) + i0) = Y[q];
+    } else {
+      const float fp = cxq(q) > 0 && xl.edge_prev && prev_in ? xs_last[wprev][q] : 0.f;
+      const float fn = cxq(q) < 0 && xl.edge_next && next_in ? xs_first[wnext][q - 9] : 0.f;
+      shift_out_f32(Y[q], cxq(q), a.p[q] + row_out(cyq(q), czq(q)), i0, i_prev, i_next, xl, prev_in, next_in, fp,
+                    fn);
     }
   }
 }
@@ -1045,6 +1243,18 @@ static cudaError_t two_impl(const Lattice& s, const Lattice& d, const StepK& K, 
   Pops<S> pd = pops_of<S>(d);
   pd.p[Q - 1] = (S*)s.p[Q - 1];  // pop 19 in place (SRC/col_MC.F90:351)
   Shape sh = cell_shape(s.g);
+  // FP32: two cells per thread where the box fits it (automatic or 2): on
+  // B200 at 256^3, 43.7 GLUPS against 42.0 with one cell per thread, the
+  // Smagorinsky step 43.5 against 40.7
+  const int lt2 = F::id == FORM_F32 && (variant == 0 || variant == 2) ? f16v_log_tpr(s.g, 2) : -1;
+  if (lt2 >= 0) {
+    Pops<float> pf = pops_of<float>(d);
+    pf.p[Q - 1] = (float*)s.p[Q - 1];
+    const dim3 grid = f16v_grid(s.g, lt2, s.g.nz);
+    if (K.les) k_two_f32v<true><<<grid, 128, 0, st>>>(pops_of<const float>(s), pf, s.g, K, lt2, 0);
+    else k_two_f32v<false><<<grid, 128, 0, st>>>(pops_of<const float>(s), pf, s.g, K, lt2, 0);
+    return cudaGetLastError();
+  }
   if (K.les) {  // the Smagorinsky collision: one cell per thread, FP16 four where the box fits
     const int lt = F::id == FORM_F16 && (variant == 0 || variant == 4) ? f16v_log_tpr(s.g, 4) : -1;
     if (lt >= 0) {
@@ -1062,8 +1272,8 @@ static cudaError_t two_impl(const Lattice& s, const Lattice& d, const StepK& K, 
     cudaError_t e = launch_rows(s, d, ROW_TWO, K, st, &launched);
     if (e != cudaSuccess || launched) return e;
   }
-  // automatic choice (variant 0): one cell per thread for FP64 and FP32, four
-  // cells per thread for FP16 where the box fits it - the fastest measured on
+  // automatic choice (variant 0): one cell per thread for FP64, two for FP32
+  // (above), four cells per thread for FP16 where the box fits it - the fastest measured on
   // B200 at 256^3 (FP16: 76.6 GLUPS with four cells per thread against 64.0
   // with one, 62.7 with two and 44.6 for the row pipeline)
   if (F::id == FORM_F16 && (variant == 2 || variant == 4 || variant == 0)) {
@@ -1113,6 +1323,23 @@ static cudaError_t aa_impl(const Lattice& a, int odd, const StepK& K, int varian
   using S = typename F::S;
   Shape sh = cell_shape(a.g);
   const int lt4 = F::id == FORM_F16 && (variant == 0 || variant == 4) ? f16v_log_tpr(a.g, 4) : -1;
+  // FP32: two cells per thread where the box fits it (automatic or 2): on
+  // B200 the pair of AA steps measured 41.9 GLUPS against 39.8 with one cell
+  // per thread at 256^3 (40.5 against 38.9 at 1024^3), the Smagorinsky pair
+  // 40.6 against 34.1
+  const int lt2 = F::id == FORM_F32 && (variant == 0 || variant == 2) ? f16v_log_tpr(a.g, 2) : -1;
+  if (lt2 >= 0) {
+    const dim3 grid = f16v_grid(a.g, lt2, a.g.nz);
+    Pops<float> pf = pops_of<float>(a);
+    if (K.les) {
+      if (odd) k_aa_f32v<true, true><<<grid, 128, 0, st>>>(pf, a.g, K, lt2);
+      else k_aa_f32v<false, true><<<grid, 128, 0, st>>>(pf, a.g, K, lt2);
+    } else {
+      if (odd) k_aa_f32v<true, false><<<grid, 128, 0, st>>>(pf, a.g, K, lt2);
+      else k_aa_f32v<false, false><<<grid, 128, 0, st>>>(pf, a.g, K, lt2);
+    }
+    return cudaGetLastError();
+  }
   if (K.les) {
     if (lt4 >= 0) {
       const dim3 grid = f16v_grid(a.g, lt4, a.g.nz);
@@ -1313,11 +1540,18 @@ static cudaError_t slab_impl(const Lattice& s, const Lattice& d, const StepK& K,
   if (K.les) k_slab<F, true, true><<<ge, sh.block, 0, st>>>(ps, pd, s.g, K, h);
   else k_slab<F, false, true><<<ge, sh.block, 0, st>>>(ps, pd, s.g, K, h);
   if (s.g.nz > 2) {
-    // FP16: the interior planes on the four-cells-per-thread kernel where the
-    // rows fit it (planes 1 .. nz-2 pull only inside the slab, so its z wrap
-    // never applies)
+    // FP16 / FP32: the interior planes on the four- / two-cells-per-thread
+    // kernel where the rows fit it (planes 1 .. nz-2 pull only inside the
+    // slab, so its z wrap never applies)
     const int lt = F::id == FORM_F16 ? f16v_log_tpr(s.g, 4) : -1;
-    if (lt >= 0) {
+    const int lt2 = F::id == FORM_F32 ? f16v_log_tpr(s.g, 2) : -1;
+    if (lt2 >= 0) {
+      Pops<float> pf = pops_of<float>(d);
+      pf.p[Q - 1] = (float*)s.p[Q - 1];
+      const dim3 gv = f16v_grid(s.g, lt2, s.g.nz - 2);
+      if (K.les) k_two_f32v<true><<<gv, 128, 0, st_in>>>(pops_of<const float>(s), pf, s.g, K, lt2, 1);
+      else k_two_f32v<false><<<gv, 128, 0, st_in>>>(pops_of<const float>(s), pf, s.g, K, lt2, 1);
+    } else if (lt >= 0) {
       Pops<__half> ph = pops_of<__half>(d);
       ph.p[Q - 1] = (__half*)s.p[Q - 1];
       const dim3 gv = f16v_grid(s.g, lt, s.g.nz - 2);

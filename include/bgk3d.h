@@ -89,20 +89,21 @@ typedef struct {
   int use_omega;       /* 1: use `omega` below instead of the svisc formula */
   double omega;        /* collision frequency override (e.g. 0 = pure streaming) */
   int extras;          /* 1: bgk_diagnostic also computes enstrophy */
-  int kernel;          /* stream-collide kernel: 0 automatic (FP16 two-lattice: 4 where
-                          the box fits, else 1), 1 one cell per thread,
-                          2 / 4 two / four cells per thread (FP16 two-lattice), 8 row
-                          pipeline with TMA bulk copies into shared memory (rows up to
-                          about 5 KB); boxes a kernel does not fit use 1. All give
-                          identical results. */
+  int kernel;          /* stream-collide kernel: 0 automatic (FP16: 4 where the box
+                          fits, FP32: 2 where it fits, else 1), 1 one cell per thread,
+                          2 two cells per thread (FP32 both schemes, FP16 two-lattice),
+                          4 four cells per thread (FP16), 8 row pipeline with TMA bulk
+                          copies into shared memory (rows up to about 5 KB); boxes a
+                          kernel does not fit use 1. All give identical results. */
   double les_cs;       /* Smagorinsky constant cteS (SRC/input.F90:47, SRC/storage.F90:87).
                           > 0 enables the LES collision of SRC/col_MC.F90:221-309 (the
                           block the reference compiles under -DLES and then stops in):
                           per cell Ptotal = |Pi_neq|, Ts = 1/(2 omega) +
                           sqrt(18 cteS^2 Ptotal + (1/omega)^2)/2, relaxation with 1/Ts.
                           0 (default) = plain BGK. The LES collision runs on the one
-                          cell per thread kernels, and in FP16 on the four cells per
-                          thread kernels where the box fits (kernel 2/8 fall back);
+                          cell per thread kernels, in FP32 on the two and in FP16 on
+                          the four cells per thread kernels where the box fits (FP16
+                          kernel 2 and kernel 8 fall back);
                           bgk_adjoint and bgk_tangent reject it. */
   int proc_z;          /* number of z-slabs the box is split into (the reference's
                           proc_z, SRC/input.F90:41; proc_x = proc_y = 1). 1 (default):

@@ -3,9 +3,10 @@ reference's -DLES block of SRC/col_MC.F90:221-309, through the C-ABI.
 
 Tolerance: bit-exact against the oracle in all three forms and both schemes
 (the kernels round every operation, square roots included, as the oracle
-does), with the FP16 four-cells-per-thread kernels where a box fits them
-(rows inside a warp, one and two warps per row); kernel choices 2/8 fall back
-to the one cell per thread kernels and give the same bits."""
+does), with the FP16 four-cells-per-thread and FP32 two-cells-per-thread
+kernels where a box fits them (rows inside a warp, one and several warps per
+row); in FP16 kernel choices 2/8 fall back to the one cell per thread kernels
+and give the same bits."""
 import numpy as np
 import pytest
 
@@ -39,6 +40,23 @@ def _pair(bgk, O, shape, form, scheme, cs, svisc, init, kernel=0):
 def test_les_bitexact_vs_oracle(bgk, oracle_mod, form, scheme, case):
     init, shape, cs = case
     orc, box = _pair(bgk, oracle_mod, shape, form, scheme, cs, 1e-4, init)
+    for it in range(1, 8):
+        orc.step(1e-4, periodic=True)
+        box.col_MC(it)
+        if it in (1, 2, 7):
+            assert same_bits(box.populations(), orc.get_pops()), f"after {it} steps"
+    box.close()
+
+
+@pytest.mark.parametrize("kernel", [0, 2])
+@pytest.mark.parametrize("case", [("tgv", (33, 20, 7), 0.17), ("hit", (16, 16, 16), 1.0), ("tgv", (128, 8, 6), 0.17),
+                                  ("tgv", (512, 4, 3), 1.0)])
+@pytest.mark.parametrize("scheme", ["two_lattice", "aa"])
+def test_les_fp32_kernels_bitexact(bgk, oracle_mod, kernel, case, scheme):
+    """The FP32 Smagorinsky steps with two cells per thread (and their
+    fallback where a box does not fit) give the oracle's bits."""
+    init, shape, cs = case
+    orc, box = _pair(bgk, oracle_mod, shape, "fp32", scheme, cs, 1e-4, init, kernel=kernel)
     for it in range(1, 8):
         orc.step(1e-4, periodic=True)
         box.col_MC(it)

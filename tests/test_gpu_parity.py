@@ -84,6 +84,39 @@ def test_fp16_kernel_variants_bitexact(bgk, oracle_mod, kernel, shape):
     box.close()
 
 
+@pytest.mark.parametrize("kernel", [0, 1, 2])
+@pytest.mark.parametrize("shape", [(64, 64, 64), (32, 16, 8), (8, 8, 8), (256, 4, 4), (128, 6, 5), (24, 8, 6),
+                                   (1024, 4, 4), (64, 3, 2)])
+def test_fp32_two_lattice_kernel_variants_bitexact(bgk, oracle_mod, kernel, shape):
+    """The two-cells-per-thread FP32 two-lattice kernel (warp-shuffle
+    x-shifts, cross-warp loads when a row spans several warps, fallback where a
+    box does not fit) gives the oracle's bits."""
+    orc, box = make_pair(bgk, oracle_mod, shape, "fp32", kernel=kernel)
+    for it in range(1, 6):
+        orc.step(0.01, periodic=True)
+        box.col_MC(it)
+        if it in (1, 5):
+            assert same_bits(box.populations(), orc.get_pops()), f"after {it} steps"
+    box.close()
+
+
+@pytest.mark.parametrize("kernel", [0, 1, 2])
+@pytest.mark.parametrize("shape", [(64, 64, 64), (32, 16, 8), (8, 8, 8), (256, 4, 4), (128, 6, 5), (24, 8, 6),
+                                   (512, 2, 3), (1024, 4, 4), (64, 3, 2), (2048, 2, 2)])
+def test_fp32_aa_kernel_variants_bitexact(bgk, oracle_mod, kernel, shape):
+    """The two-cells-per-thread FP32 AA kernels (rows inside a warp, one,
+    two and four warps per row, rows over two and four blocks, blocks with
+    idle warps, fallback where a box does not fit) give the oracle's bits
+    over steps of both parities."""
+    orc, box = make_pair(bgk, oracle_mod, shape, "fp32", scheme="aa", kernel=kernel)
+    for it in range(1, 6):
+        orc.step(0.01, periodic=True)
+        box.col_MC(it)
+        if it in (1, 2, 5):
+            assert same_bits(box.populations(), orc.get_pops()), f"after {it} steps"
+    box.close()
+
+
 @pytest.mark.parametrize("kernel", [0, 1, 4])
 @pytest.mark.parametrize("shape", [(64, 64, 64), (32, 16, 8), (8, 8, 8), (256, 4, 4), (128, 6, 5), (24, 8, 6),
                                    (512, 2, 3)])

@@ -29,7 +29,7 @@ def _kw(form, **kw):
 @pytest.mark.parametrize("form", ["fp64", "fp32", "fp16"])
 @pytest.mark.parametrize("proc_z", [2, 3, 4])
 @pytest.mark.parametrize("les_cs", [0.0, 0.17])
-@pytest.mark.parametrize("nx", [20, 32])  # 32: FP16 interior planes on the four-cells-per-thread kernel
+@pytest.mark.parametrize("nx", [20, 32])  # 32: FP16 / FP32 interior planes on the four- / two-cells-per-thread kernels
 def test_local_slabs_bitexact_vs_whole_box(bgk, form, proc_z, les_cs, nx):
     from bgk3d_hit_b200.slabs import LocalSlabs
 

@@ -186,6 +186,10 @@ def kernel_key(precision, scheme, L, kernel=0, les=False):
     """Name of the stream-collide kernel a launch runs (the key of
     profiles/ncu_traffic.json)."""
     kern = f"{'k_two' if scheme == 'two_lattice' else 'k_aa'}_{precision}" + ("_les" if les else "")
+    if precision == "fp32" and kernel in (0, 2):  # two cells per thread, both schemes, BGK and LES
+        tpr = L // 2
+        if L % 2 == 0 and tpr & (tpr - 1) == 0 and (L * tpr) % 32 == 0:
+            return ("k_two_f32v" if scheme == "two_lattice" else "k_aa_f32v") + ("_les" if les else "")
     allowed = (0, 4) if (les or scheme == "aa") else (0, 2, 4)  # the LES collision runs on four cells only
     if precision == "fp16" and kernel in allowed:
         v = 2 if kernel == 2 else 4

@@ -142,10 +142,11 @@ __device__ __forceinline__ void collide4_f16(uint2 (&Y)[Q], const StepK& K) {
   }
 }
 
-// Lanes that exchange x-neighbours in the four-cells-per-thread FP16 kernels:
-// a row of nx cells is tpr = nx/4 consecutive threads. Rows shorter than a warp
-// wrap inside it; rows of one or more warps wrap through global memory at the
-// warp's first / last lane (edge_prev / edge_next).
+// Lanes that exchange x-neighbours in the several-cells-per-thread kernels:
+// a row of nx cells is tpr = nx/V consecutive threads (V cells per thread).
+// Rows shorter than a warp wrap inside it; rows of one or more warps wrap
+// through global memory at the warp's first / last lane (edge_prev /
+// edge_next).
 struct XLanes {
   int src_prev, src_next;
   bool edge_prev, edge_next;
@@ -263,8 +264,9 @@ __global__ void __launch_bounds__(128, 5) k_two_f32v(Pops<const float> src, Pops
   for (int q = 0; q < Q; ++q) {
     const int jj = cyq(q) > 0 ? jm : (cyq(q) < 0 ? jp : j);
     const int kk = czq(q) > 0 ? km : (czq(q) < 0 ? kp : k);
-    // pop 19 in place (src.p[18] == dst.p[18]) with a plain load
-    const float* p = (q == Q - 1 ? (const float*)dst.p[Q - 1] : src.p[q]) + g.sx * (jj + g.ny * kk);
+    // pop 19 with a plain load: in the time loop it is updated in place
+    // (src.p[18] == dst.p[18]); the adjoint's out-of-place steps pass distinct arrays
+    const float* p = src.p[q] + g.sx * (jj + g.ny * kk);
     Y[q] = (q == Q - 1) ? *reinterpret_cast<const float2*>(p + i0) : __ldg(reinterpret_cast<const float2*>(p + i0));
     E[q] = 0.f;
     if (cxq(q) > 0 && xl.edge_prev) E[q] = __ldg(p + i_prev);
@@ -1219,14 +1221,15 @@ StepK make_stepk(int form, double omega, double scale, double les_cs) {
   return k;
 }
 
-// Grid of the FP16 vector kernels: 128-thread blocks over the ny * 2^log_tpr
-// threads of a plane, `planes` planes.
-static dim3 f16v_grid(const Geo& g, int log_tpr, int planes) {
+// Grid of the several-cells-per-thread kernels: 128-thread blocks over the
+// ny * 2^log_tpr threads of a plane, `planes` planes.
+static dim3 vec_grid(const Geo& g, int log_tpr, int planes) {
   return dim3((unsigned)((((long long)g.ny << log_tpr) + 127) / 128), (unsigned)planes);
 }
 
-// log2(nx/V) when the V-cells-per-thread FP16 kernel applies, else -1.
-static int f16v_log_tpr(const Geo& g, int V) {
+// log2(nx/V) when a V-cells-per-thread kernel applies (nx/V a power of two,
+// whole warps per plane), else -1.
+static int vec_log_tpr(const Geo& g, int V) {
   if (g.nx % V) return -1;
   const int tpr = g.nx / V;
   if (tpr & (tpr - 1)) return -1;
@@ -1246,21 +1249,21 @@ static cudaError_t two_impl(const Lattice& s, const Lattice& d, const StepK& K, 
   // FP32: two cells per thread where the box fits it (automatic or 2): on
   // B200 at 256^3, 43.7 GLUPS against 42.0 with one cell per thread, the
   // Smagorinsky step 43.5 against 40.7
-  const int lt2 = F::id == FORM_F32 && (variant == 0 || variant == 2) ? f16v_log_tpr(s.g, 2) : -1;
+  const int lt2 = F::id == FORM_F32 && (variant == 0 || variant == 2) ? vec_log_tpr(s.g, 2) : -1;
   if (lt2 >= 0) {
     Pops<float> pf = pops_of<float>(d);
     pf.p[Q - 1] = (float*)s.p[Q - 1];
-    const dim3 grid = f16v_grid(s.g, lt2, s.g.nz);
+    const dim3 grid = vec_grid(s.g, lt2, s.g.nz);
     if (K.les) k_two_f32v<true><<<grid, 128, 0, st>>>(pops_of<const float>(s), pf, s.g, K, lt2, 0);
     else k_two_f32v<false><<<grid, 128, 0, st>>>(pops_of<const float>(s), pf, s.g, K, lt2, 0);
     return cudaGetLastError();
   }
   if (K.les) {  // the Smagorinsky collision: one cell per thread, FP16 four where the box fits
-    const int lt = F::id == FORM_F16 && (variant == 0 || variant == 4) ? f16v_log_tpr(s.g, 4) : -1;
+    const int lt = F::id == FORM_F16 && (variant == 0 || variant == 4) ? vec_log_tpr(s.g, 4) : -1;
     if (lt >= 0) {
       Pops<__half> ph = pops_of<__half>(d);
       ph.p[Q - 1] = (__half*)s.p[Q - 1];
-      const dim3 grid = f16v_grid(s.g, lt, s.g.nz);
+      const dim3 grid = vec_grid(s.g, lt, s.g.nz);
       k_two_f16v<true><<<grid, 128, 0, st>>>(pops_of<const __half>(s), ph, s.g, K, lt, 0);
     } else {
       k_two<F, true><<<sh.grid, sh.block, 0, st>>>(ps, pd, s.g, K);
@@ -1278,7 +1281,7 @@ static cudaError_t two_impl(const Lattice& s, const Lattice& d, const StepK& K, 
   // with one, 62.7 with two and 44.6 for the row pipeline)
   if (F::id == FORM_F16 && (variant == 2 || variant == 4 || variant == 0)) {
     const int V = variant == 0 ? 4 : variant;
-    const int lt = f16v_log_tpr(s.g, V);
+    const int lt = vec_log_tpr(s.g, V);
     if (lt >= 0) {
       const long long threads = (long long)s.g.ny << lt;
       dim3 grid((unsigned)((threads + (V == 4 ? 127 : 255)) / (V == 4 ? 128 : 256)), s.g.nz);
@@ -1300,9 +1303,15 @@ cudaError_t launch_step_out_of_place(const Lattice& src, const Lattice& dst, dou
     case FORM_F64:
       k_two<F64><<<sh.grid, sh.block, 0, st>>>(pops_of<const double>(src), pops_of<double>(dst), src.g, K);
       return cudaGetLastError();
-    case FORM_F32:
-      k_two<F32><<<sh.grid, sh.block, 0, st>>>(pops_of<const float>(src), pops_of<float>(dst), src.g, K);
+    case FORM_F32: {
+      const int lt2 = vec_log_tpr(src.g, 2);
+      if (lt2 >= 0)
+        k_two_f32v<false><<<vec_grid(src.g, lt2, src.g.nz), 128, 0, st>>>(pops_of<const float>(src),
+                                                                           pops_of<float>(dst), src.g, K, lt2, 0);
+      else
+        k_two<F32><<<sh.grid, sh.block, 0, st>>>(pops_of<const float>(src), pops_of<float>(dst), src.g, K);
       return cudaGetLastError();
+    }
   }
   return cudaErrorInvalidValue;
 }
@@ -1322,14 +1331,14 @@ template <class F>
 static cudaError_t aa_impl(const Lattice& a, int odd, const StepK& K, int variant, cudaStream_t st) {
   using S = typename F::S;
   Shape sh = cell_shape(a.g);
-  const int lt4 = F::id == FORM_F16 && (variant == 0 || variant == 4) ? f16v_log_tpr(a.g, 4) : -1;
+  const int lt4 = F::id == FORM_F16 && (variant == 0 || variant == 4) ? vec_log_tpr(a.g, 4) : -1;
   // FP32: two cells per thread where the box fits it (automatic or 2): on
   // B200 the pair of AA steps measured 41.9 GLUPS against 39.8 with one cell
   // per thread at 256^3 (40.5 against 38.9 at 1024^3), the Smagorinsky pair
   // 40.6 against 34.1
-  const int lt2 = F::id == FORM_F32 && (variant == 0 || variant == 2) ? f16v_log_tpr(a.g, 2) : -1;
+  const int lt2 = F::id == FORM_F32 && (variant == 0 || variant == 2) ? vec_log_tpr(a.g, 2) : -1;
   if (lt2 >= 0) {
-    const dim3 grid = f16v_grid(a.g, lt2, a.g.nz);
+    const dim3 grid = vec_grid(a.g, lt2, a.g.nz);
     Pops<float> pf = pops_of<float>(a);
     if (K.les) {
       if (odd) k_aa_f32v<true, true><<<grid, 128, 0, st>>>(pf, a.g, K, lt2);
@@ -1342,7 +1351,7 @@ static cudaError_t aa_impl(const Lattice& a, int odd, const StepK& K, int varian
   }
   if (K.les) {
     if (lt4 >= 0) {
-      const dim3 grid = f16v_grid(a.g, lt4, a.g.nz);
+      const dim3 grid = vec_grid(a.g, lt4, a.g.nz);
       if (odd) k_aa_f16v<true, true><<<grid, 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
       else k_aa_f16v<false, true><<<grid, 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
     } else if (odd) {
@@ -1359,7 +1368,7 @@ static cudaError_t aa_impl(const Lattice& a, int odd, const StepK& K, int varian
   }
   // FP16: four cells per thread where the box fits it (automatic or 4)
   if (lt4 >= 0) {
-    const dim3 grid = f16v_grid(a.g, lt4, a.g.nz);
+    const dim3 grid = vec_grid(a.g, lt4, a.g.nz);
     if (odd) k_aa_f16v<true, false><<<grid, 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
     else k_aa_f16v<false, false><<<grid, 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt4);
     return cudaGetLastError();
@@ -1543,18 +1552,18 @@ static cudaError_t slab_impl(const Lattice& s, const Lattice& d, const StepK& K,
     // FP16 / FP32: the interior planes on the four- / two-cells-per-thread
     // kernel where the rows fit it (planes 1 .. nz-2 pull only inside the
     // slab, so its z wrap never applies)
-    const int lt = F::id == FORM_F16 ? f16v_log_tpr(s.g, 4) : -1;
-    const int lt2 = F::id == FORM_F32 ? f16v_log_tpr(s.g, 2) : -1;
+    const int lt = F::id == FORM_F16 ? vec_log_tpr(s.g, 4) : -1;
+    const int lt2 = F::id == FORM_F32 ? vec_log_tpr(s.g, 2) : -1;
     if (lt2 >= 0) {
       Pops<float> pf = pops_of<float>(d);
       pf.p[Q - 1] = (float*)s.p[Q - 1];
-      const dim3 gv = f16v_grid(s.g, lt2, s.g.nz - 2);
+      const dim3 gv = vec_grid(s.g, lt2, s.g.nz - 2);
       if (K.les) k_two_f32v<true><<<gv, 128, 0, st_in>>>(pops_of<const float>(s), pf, s.g, K, lt2, 1);
       else k_two_f32v<false><<<gv, 128, 0, st_in>>>(pops_of<const float>(s), pf, s.g, K, lt2, 1);
     } else if (lt >= 0) {
       Pops<__half> ph = pops_of<__half>(d);
       ph.p[Q - 1] = (__half*)s.p[Q - 1];
-      const dim3 gv = f16v_grid(s.g, lt, s.g.nz - 2);
+      const dim3 gv = vec_grid(s.g, lt, s.g.nz - 2);
       if (K.les) k_two_f16v<true><<<gv, 128, 0, st_in>>>(pops_of<const __half>(s), ph, s.g, K, lt, 1);
       else k_two_f16v<false><<<gv, 128, 0, st_in>>>(pops_of<const __half>(s), ph, s.g, K, lt, 1);
     } else {

@@ -223,11 +223,10 @@ __global__ void __launch_bounds__(128, 5) k_two_f16v(Pops<const __half> src, Pop
   for (int q = 0; q < Q; ++q) *reinterpret_cast<uint2*>(dst.p[q] + o) = Y[q];
 }
 
-// FP32 two-lattice step with 2 cells per thread and 8-byte accesses (tpr =
-// nx/2 threads per row): k_two_f16v's row split and x-crossing shuffles on
-// chunks of two floats, F32::cell's arithmetic on each cell, so the results
-// are those of k_two<F32>.
-// x-shifted rows of two-float chunks: shift_rows on FP32 pairs.
+// Second half of the x-shifted row loads of the two-cells-per-thread FP32
+// kernels: shift_rows on chunks of two floats (Y[q] holds elements i0, i0+1;
+// the element that crosses the chunk comes from the neighbouring lane or, for
+// a warp's edge lane, from E[q]).
 __device__ __forceinline__ void shift_rows_f32(float2 (&Y)[Q], const float (&E)[Q], const XLanes& xl) {
 #pragma unroll
   for (int q = 0; q < Q; ++q) {
@@ -244,6 +243,11 @@ __device__ __forceinline__ void shift_rows_f32(float2 (&Y)[Q], const float (&E)[
   }
 }
 
+// FP32 two-lattice step with 2 cells per thread and 8-byte accesses (tpr =
+// nx/2 threads per row): k_two_f16v's row split and x-crossing shuffles on
+// chunks of two floats, F32::cell's arithmetic on each cell, so the results
+// are those of k_two<F32>. 72 registers (80 for the Smagorinsky step), no
+// spills.
 template <bool LES>
 __global__ void __launch_bounds__(128, 5) k_two_f32v(Pops<const float> src, Pops<float> dst, Geo g, StepK K,
                                                   int log_tpr, int k0) {
@@ -290,7 +294,8 @@ __global__ void __launch_bounds__(128, 5) k_two_f32v(Pops<const float> src, Pops
   for (int q = 0; q < Q; ++q) *reinterpret_cast<float2*>(dst.p[q] + o) = Y[q];
 }
 
-// Same with 2 cells per thread and 4-byte accesses (tpr = nx/2 threads per row).
+// FP16 two-lattice step with 2 cells per thread and 4-byte accesses (tpr =
+// nx/2 threads per row); otherwise as k_two_f16v.
 __global__ void __launch_bounds__(256, 4) k_two_f16v2(Pops<const __half> src, Pops<__half> dst, Geo g, StepK K,
                                                    int log_tpr) {
   const int tpr = 1 << log_tpr;
@@ -570,11 +575,6 @@ __global__ void __launch_bounds__(128, 5) k_aa_f16v(Pops<__half> a, Geo g, StepK
   }
 }
 
-// FP32 AA pattern with two cells per thread: k_aa_f16v's row split (tpr =
-// nx/2 threads per row), x-crossing shuffles and block-local warp-edge stores
-// on 8-byte chunks of two floats, F32::cell's arithmetic (the reference's
-// order) on each cell, so the results are those of k_aa<F32, ODD>. The same
-// ownership argument keeps the in-place update race-free.
 // Store side of the FP32 odd step: cells i0, i0+1 go to elements i0 + cx,
 // i0 + 1 + cx of row p, stored as the aligned chunk (i0, i0+1) completed with
 // the neighbouring lane's crossing value, as shift_out does for FP16.
@@ -598,6 +598,12 @@ __device__ __forceinline__ void shift_out_f32(float2 Y, int cx, float* p, int i0
   }
 }
 
+// FP32 AA pattern with two cells per thread: k_aa_f16v's row split (tpr =
+// nx/2 threads per row), x-crossing shuffles and block-local warp-edge stores
+// on 8-byte chunks of two floats, F32::cell's arithmetic (the reference's
+// order) on each cell, so the results are those of k_aa<F32, ODD>. The same
+// ownership argument keeps the in-place update race-free. 95 registers (87
+// for the Smagorinsky even step), no spills.
 template <bool ODD, bool LES>
 __global__ void __launch_bounds__(128, 5) k_aa_f32v(Pops<float> a, Geo g, StepK K, int log_tpr) {
   const int tpr = 1 << log_tpr;

@@ -5,6 +5,11 @@
 //                replaces the halo exchange of SRC/bcond.comm.step3.F90
 //   k_aa         in-place AA-pattern variant of the same update (no reference
 //                counterpart; same per-cell arithmetic)
+//   k_two_f32v, k_aa_f32v / k_two_f16v, k_aa_f16v
+//                the same updates with two FP32 / four FP16 cells of a row per
+//                thread (8-byte accesses, x-crossing values by warp shuffle);
+//                the defaults of those forms where a box fits them
+//   k_slab       two-lattice step of one z-slab with the face exchange fused in
 //   k_init_*     equilibrium initial conditions (SRC/init.F90:83-141)
 //   k_diag       diagno + dissipation + strain-rate sums (SRC/diagno.F90:73-121,
 //                SRC/dissipation.F90:65-269) as deterministic compensated

@@ -43,7 +43,10 @@ int cuda_fail(cudaError_t e, const char* what) {
 constexpr int ROW_ALIGN = 32;
 constexpr long long POP_ALIGN = 256;
 // Staging for host velocity input: this many cells per chunk (whole planes).
-constexpr long long INIT_CHUNK_CELLS = 1LL << 24;
+// Cells per chunk of a velocity-field upload from host memory: two staging
+// sets of three such chunks (96 MB) let the copy of one chunk run beside the
+// initialisation kernel of the previous one.
+constexpr long long INIT_CHUNK_CELLS = 1LL << 21;
 
 }  // namespace
 
@@ -80,6 +83,9 @@ struct bgk_ctx {
   void* vel = nullptr;
   void* stage = nullptr;
   size_t stage_bytes = 0;
+  // host upload pipeline: copy stream, staging set filled / free again
+  cudaStream_t st_copy = nullptr;
+  cudaEvent_t ev_full[2] = {nullptr, nullptr}, ev_free[2] = {nullptr, nullptr};
   long long launches = 0;
   long long dev_bytes = 0;
   void* fft_buf = nullptr;
@@ -264,11 +270,18 @@ int init_velocity_impl(bgk_ctx* c, const double* u, const double* v, const doubl
   const size_t chunk = (size_t)plane * nk;
   double *su = nullptr, *sv = nullptr, *sw = nullptr;
   if (!on_device) {
-    rc = ensure_stage(c, 3 * chunk * sizeof(double));
+    // two staging sets of three chunks; the copies run on their own stream
+    rc = ensure_stage(c, 2 * 3 * chunk * sizeof(double));
     if (rc) return rc;
-    su = (double*)c->stage;
-    sv = su + chunk;
-    sw = sv + chunk;
+    if (!c->st_copy) CK(cudaStreamCreateWithFlags(&c->st_copy, cudaStreamNonBlocking));
+    for (int b = 0; b < 2; ++b) {
+      if (!c->ev_full[b]) CK(cudaEventCreateWithFlags(&c->ev_full[b], cudaEventDisableTiming));
+      if (!c->ev_free[b]) CK(cudaEventCreateWithFlags(&c->ev_free[b], cudaEventDisableTiming));
+    }
+    // nothing queued on the context's stream before this call may still
+    // read a staging set when the first copies land
+    CK(cudaEventRecord(c->ev_free[0], c->st));
+    CK(cudaEventRecord(c->ev_free[1], c->st));
   }
   const int lay = init_layout(c);
   const bool measure = c->form == FORM_F16 && c->p.fp16_scale == 0.0;
@@ -278,7 +291,8 @@ int init_velocity_impl(bgk_ctx* c, const double* u, const double* v, const doubl
       rc = set_scale_from_max(c);
       if (rc) return rc;
     }
-    for (int k0 = 0; k0 < c->g.nz; k0 += nk) {
+    int set = 0;  // staging set of this chunk
+    for (int k0 = 0; k0 < c->g.nz; k0 += nk, set ^= 1) {
       const int nkk = k0 + nk <= c->g.nz ? nk : c->g.nz - k0;
       const size_t off = (size_t)plane * k0, cnt = (size_t)plane * nkk * sizeof(double);
       if (on_device) {
@@ -286,12 +300,21 @@ int init_velocity_impl(bgk_ctx* c, const double* u, const double* v, const doubl
         sv = const_cast<double*>(v) + off;
         sw = const_cast<double*>(w) + off;
       } else {
-        CK(cudaMemcpyAsync(su, u + off, cnt, cudaMemcpyHostToDevice, c->st));
-        CK(cudaMemcpyAsync(sv, v + off, cnt, cudaMemcpyHostToDevice, c->st));
-        CK(cudaMemcpyAsync(sw, w + off, cnt, cudaMemcpyHostToDevice, c->st));
+        // copy into this set once the kernel that read it two chunks ago is
+        // done, while the context's stream initialises the previous chunk
+        su = (double*)c->stage + (size_t)set * 3 * chunk;
+        sv = su + chunk;
+        sw = sv + chunk;
+        CK(cudaStreamWaitEvent(c->st_copy, c->ev_free[set], 0));
+        CK(cudaMemcpyAsync(su, u + off, cnt, cudaMemcpyHostToDevice, c->st_copy));
+        CK(cudaMemcpyAsync(sv, v + off, cnt, cudaMemcpyHostToDevice, c->st_copy));
+        CK(cudaMemcpyAsync(sw, w + off, cnt, cudaMemcpyHostToDevice, c->st_copy));
+        CK(cudaEventRecord(c->ev_full[set], c->st_copy));
+        CK(cudaStreamWaitEvent(c->st, c->ev_full[set], 0));
       }
       CK(launch_init_velocity(c->A, lay, su, sv, sw, rho, k0, nkk, pass == 0 ? 1.0 : c->scale,
                               pass == 0 ? c->d_max : nullptr, c->st));
+      if (!on_device) CK(cudaEventRecord(c->ev_free[set], c->st));
       c->launches++;
     }
   }
@@ -614,6 +637,11 @@ int bgk_destroy(bgk_ctx* c) {
   if (c->ev_join) cudaEventDestroy(c->ev_join);
   if (c->ev_edge0) cudaEventDestroy(c->ev_edge0);
   if (c->ev_edge1) cudaEventDestroy(c->ev_edge1);
+  for (int b = 0; b < 2; ++b) {
+    if (c->ev_full[b]) cudaEventDestroy(c->ev_full[b]);
+    if (c->ev_free[b]) cudaEventDestroy(c->ev_free[b]);
+  }
+  if (c->st_copy) cudaStreamDestroy(c->st_copy);
   if (c->st_in) cudaStreamDestroy(c->st_in);
   if (c->st) cudaStreamDestroy(c->st);
   delete c;

@@ -23,6 +23,7 @@ BGK_ERR_NONFINITE = -5
 BGK_FP64, BGK_FP32DEV, BGK_FP16DEV = 0, 1, 2
 BGK_TWO_LATTICE, BGK_AA = 0, 1
 BGK_CORRECTED, BGK_FAITHFUL = 0, 1
+BGK_ADJ_RECOMPUTE, BGK_ADJ_REBUILD = 0, 1
 
 PRECISIONS = {"fp64": BGK_FP64, "fp32": BGK_FP32DEV, "fp16": BGK_FP16DEV}
 SCHEMES = {"two_lattice": BGK_TWO_LATTICE, "aa": BGK_AA}
@@ -80,6 +81,8 @@ PROTOTYPES = [
     ("bgk_vtk", _i, [_vp, _i, _i, _i, C.c_char_p]),
     ("bgk_adjoint", _i, [_vp, _dp, _dp, _dp, _dp, _dp, _dp, _i, _i, _dp, _dp, _dp]),
     ("bgk_adjoint_cache", _i, [_vp, C.c_size_t]),
+    ("bgk_adjoint_mode", _i, [_vp, _i]),
+    ("bgk_adjoint_rebuilds", _i, [_d, _i]),
     ("bgk_tangent", _i, [_vp, _dp, _dp, _dp, _dp, _dp, _dp, _d, _dp, _dp, _dp, _i, _dp, _dp]),
     ("bgk_get_scale", _i, [_vp, _dp]),
     ("bgk_get_omega", _i, [_vp, _dp]),

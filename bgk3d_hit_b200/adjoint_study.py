@@ -2,6 +2,7 @@
 
     python -m bgk3d_hit_b200.adjoint_study [--size 128] [--steps 1000] [--ckpt 32]
         [--tau 0.51] [--k0 4] [--dirs 64] [--h 1e-6] [--precision fp64] [--cache-gb 0]
+        [--mode recompute|rebuild]
 
 Initial velocity: seeded HIT field (seed 1234, E(k) ~ k^4 exp(-2 (k/k0)^2),
 u_rms = 0.03); target u_tgt: the same generator with a second seed (4321).
@@ -19,7 +20,11 @@ Loss = 0.5 mean |u(T) - u_tgt|^2. Reports, as one JSON object:
   backward) over the wall time of a forward-only call of the same length
   (medians of 5 calls each);
   with --cache-gb G, bgk_adjoint keeps up to G GB of forward states between
-  checkpoints instead of recomputing them (bgk_adjoint_cache);
+  checkpoints instead of recomputing them (bgk_adjoint_cache); with
+  --mode rebuild the backward pass rebuilds the states between checkpoints
+  from the one after them (bgk_adjoint_mode BGK_ADJ_REBUILD), and
+  vs_recompute gives the relative L2 difference of its gradient from the
+  recomputing mode's;
 - vs_fp64 (FP32 storage only): the relative L2 difference between the FP32
   gradient and the FP64 adjoint gradient of the same problem (central
   differences of an FP32 loss over 1000 steps are dominated by its rounding,
@@ -34,6 +39,7 @@ import time
 
 import numpy as np
 
+from . import _abi
 from .hit import hit_velocity
 from .solver import BGK3D
 
@@ -56,13 +62,17 @@ def _adj(box, u0, ut, T, K, grads):
 
 
 def run(size=128, steps=1000, ckpt=32, tau=0.51, k0=4.0, u_rms=0.03, dirs=64, h=1e-6, precision="fp64", ntan=4,
-        cache_gb=0.0, reps=5, sweep=(1e-3, 1e-4, 1e-5, 1e-6, 1e-7)):
+        cache_gb=0.0, reps=5, sweep=(1e-3, 1e-4, 1e-5, 1e-6, 1e-7), mode="recompute"):
     svisc = (tau - 0.5) / 3.0
     u0 = [np.ascontiguousarray(a) for a in hit_velocity(size, k0, u_rms, 1234)]
     ut = [np.ascontiguousarray(a) for a in hit_velocity(size, k0, u_rms, 4321)]
     box = BGK3D(size, svisc=svisc, u0=u_rms, precision=precision)
     if cache_gb > 0:
         box._lib.bgk_adjoint_cache(box._h, int(cache_gb * 1e9))
+    if mode == "rebuild":
+        if not box._lib.bgk_adjoint_rebuilds(box.omega, ckpt):
+            raise ValueError("rebuild mode does not apply to tau %g with a checkpoint every %d steps" % (tau, ckpt))
+        box._lib.bgk_adjoint_mode(box._h, _abi.BGK_ADJ_REBUILD)
     tau_used = 1.0 / box.omega
     # cost: forward-only and full adjoint, each the median of `reps` calls
     # after one warm-up call
@@ -120,6 +130,12 @@ def run(size=128, steps=1000, ckpt=32, tau=0.51, k0=4.0, u_rms=0.03, dirs=64, h=
             raise RuntimeError(box._lib.bgk_last_error().decode())
         pred = float(np.dot(g, d.reshape(-1))) + gtau * dtau
         tan_errs.append(abs(pred - dl.value) / abs(dl.value))
+    vs_rec = None
+    if mode == "rebuild":
+        box._lib.bgk_adjoint_mode(box._h, _abi.BGK_ADJ_RECOMPUTE)
+        _, grec, gtrec = _adj(box, u0, ut, steps, ckpt, True)
+        vs_rec = {"grad_rel_l2": float(np.linalg.norm(g - grec) / np.linalg.norm(grec)),
+                  "grad_tau_rel": abs(gtau - gtrec) / abs(gtrec)}
     box.close()
     vs64 = None
     if precision != "fp64":
@@ -130,17 +146,19 @@ def run(size=128, steps=1000, ckpt=32, tau=0.51, k0=4.0, u_rms=0.03, dirs=64, h=
                 "grad_tau_rel": abs(gtau - gt64) / abs(gt64)}
     return {
         "config": {"size": size, "steps": steps, "ckpt_every": ckpt, "tau": tau_used, "k0": k0, "u_rms": u_rms,
-                   "precision": precision, "h": h, "directions": dirs, "cache_gb": cache_gb},
+                   "precision": precision, "h": h, "directions": dirs, "cache_gb": cache_gb, "mode": mode},
         "loss": loss, "loss_in_adjoint_call": loss2, "grad_tau": gtau, "fd_grad_tau": fd_tau,
-        "fd": {"max_rel_err": float(np.max(errs)), "median_rel_err": float(np.median(errs)),
-               "p90_rel_err": float(np.percentile(errs, 90)),
-               "tau_rel_err": abs(gtau - fd_tau) / abs(fd_tau)},
+        "fd": ({"max_rel_err": float(np.max(errs)), "median_rel_err": float(np.median(errs)),
+                "p90_rel_err": float(np.percentile(errs, 90)),
+                "tau_rel_err": abs(gtau - fd_tau) / abs(fd_tau)} if errs else
+               {"tau_rel_err": abs(gtau - fd_tau) / abs(fd_tau)}),
         "fd_sweep": ({"max_rel_err": float(np.max(sweep_errs)), "median_rel_err": float(np.median(sweep_errs)),
                       "p90_rel_err": float(np.percentile(sweep_errs, 90)),
                       "h_chosen": {str(x): sweep_h.count(x) for x in sorted(set(sweep_h))}} if sweep_errs else None),
-        "tangent": {"max_rel_err": float(np.max(tan_errs)), "directions": ntan},
+        "tangent": {"max_rel_err": float(np.max(tan_errs)) if tan_errs else None, "directions": ntan},
         "cost": {"forward_s": t_fwd, "adjoint_s": t_adj, "adjoint_over_forward": t_adj / t_fwd},
         "vs_fp64": vs64,
+        "vs_recompute": vs_rec,
     }
 
 
@@ -155,9 +173,11 @@ def main():
     ap.add_argument("--h", type=float, default=1e-6)
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
     ap.add_argument("--cache-gb", type=float, default=0.0)
+    ap.add_argument("--mode", default="recompute", choices=["recompute", "rebuild"])
+    ap.add_argument("--ntan", type=int, default=4)
     a = ap.parse_args()
     print(json.dumps(run(a.size, a.steps, a.ckpt, a.tau, a.k0, dirs=a.dirs, h=a.h, precision=a.precision,
-                         cache_gb=a.cache_gb)))
+                         cache_gb=a.cache_gb, mode=a.mode, ntan=a.ntan)))
 
 
 if __name__ == "__main__":

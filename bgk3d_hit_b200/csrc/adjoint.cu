@@ -190,6 +190,113 @@ __global__ void __launch_bounds__(128, 4) k_adj_step(Pops<const typename F::S> f
   }
 }
 
+// The adjoint step on a forward state rebuilt from the one after it, so that
+// the backward pass reads no stored or recomputed state between checkpoints.
+// The BGK update post = g - omega (g - e) keeps rho and j, so the
+// post-collision populations x of a cell give e = e(rho, u) and the
+// pre-collision ones g = (x - omega e) / (1 - omega); and since the state
+// after the step holds post at the cell (f_{t+1}(x) = post_t(x)),
+// sum lam.(e - g) = sum lam.(e - x) / (1 - omega). x is read unshifted from a
+// stored forward state (FIRST: the checkpoint, or the final state, that ends
+// the segment) or gathered from x + c_q of the g that the previous launch
+// rebuilt (f_{t+1}(x)_q = g_{t+1}(x + c_q)_q, as g_{t+1} is the pull of
+// f_{t+1}); lam is gathered at the same offsets. Writes mu(x) as k_adj_step
+// does and, when store_g is set, the rebuilt g(x) for the next launch. The
+// rebuilt state is the forward's up to rounding, which grows by up to
+// 1 / |1 - omega| per rebuilt step in the non-equilibrium part: the driver
+// uses this only where |1 - omega|^-(K-1) is small over a segment of K steps.
+// Moment sums in the form's arithmetic, with fused multiply-adds, like
+// k_adj_step; the dL/domega term of each cell is added in double. Register
+// caps: 3 blocks/SM for FP64 (158 registers), 8 for FP32 (64); measured
+// against 4 and 5 (FP64) and 4 and 6 (FP32), and against loading all 19
+// lam before the moment loop, all slower.
+template <class F, bool FIRST>
+__global__ void __launch_bounds__(128, F::id == 0 ? 3 : 8)
+    k_adj_inv(Pops<const typename F::S> fp, Pops<const typename F::S> lin, Pops<typename F::S> lout,
+              Pops<typename F::S> gout, int store_g, Geo g, typename F::R omega, typename F::R rinv, double* acc) {
+  using S = typename F::S; using R = typename F::R;
+  using D = R;
+  __shared__ double wsum[4];
+  double dw = 0.0;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  if (i < g.nx && j < g.ny) {
+    const int im = i == 0 ? g.nx - 1 : i - 1, ip = i == g.nx - 1 ? 0 : i + 1;
+    const int jm = j == 0 ? g.ny - 1 : j - 1, jp = j == g.ny - 1 ? 0 : j + 1;
+    const int km = k == 0 ? g.nz - 1 : k - 1, kp = k == g.nz - 1 ? 0 : k + 1;
+    const int o = i + g.sx * (j + g.ny * k);
+    auto offp = [&](int q) {  // x + c_q
+      const int ii = cxq(q) > 0 ? ip : (cxq(q) < 0 ? im : i);
+      const int jj = cyq(q) > 0 ? jp : (cyq(q) < 0 ? jm : j);
+      const int kk = czq(q) > 0 ? kp : (czq(q) < 0 ? km : k);
+      return ii + g.sx * (jj + g.ny * kk);
+    };
+    R x[Q];
+    R rho = (R)1, jx = 0, jy = 0, jz = 0;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      x[q] = (R)__ldg(fp.p[q] + (FIRST ? o : offp(q)));
+      rho += x[q];
+      jx += (R)cxq(q) * x[q];
+      jy += (R)cyq(q) * x[q];
+      jz += (R)czq(q) * x[q];
+    }
+    const R ri = (R)1 / rho;
+    const R ux = jx * ri, uy = jy * ri, uz = jz * ri;
+    const R a = (R)-1.5 * (ux * ux + uy * uy + uz * uz);
+    D L0 = 0, m1x = 0, m1y = 0, m1z = 0, mxx = 0, myy = 0, mzz = 0, mxy = 0, mxz = 0, myz = 0, S2 = 0;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      const D lam = (D)__ldg(lin.p[q] + offp(q));
+      const R cu = cdot<R>(q, ux, uy, uz);
+      const R e = wq<R>(q) * (rho * ((R)1 + a + cu * ((R)3 + (R)4.5 * cu)) - (R)1);
+      if (store_g) gout.p[q][o] = (S)((x[q] - omega * e) * rinv);
+      S2 += lam * (D)(e - x[q]);
+      const D wl = wq<D>(q) * lam;
+      L0 += wl;
+      m1x += cxq(q) * wl;
+      m1y += cyq(q) * wl;
+      m1z += czq(q) * wl;
+      mxx += (cxq(q) * cxq(q)) * wl;
+      myy += (cyq(q) * cyq(q)) * wl;
+      mzz += (czq(q) * czq(q)) * wl;
+      mxy += (cxq(q) * cyq(q)) * wl;
+      mxz += (cxq(q) * czq(q)) * wl;
+      myz += (cyq(q) * czq(q)) * wl;
+    }
+    const D nx = mxx * ux + mxy * uy + mxz * uz;  // M2 u
+    const D ny = mxy * ux + myy * uy + myz * uz;
+    const D nz = mxz * ux + myz * uy + mzz * uz;
+    const D A = L0 * ((D)1 + a) + (D)3 * (ux * m1x + uy * m1y + uz * m1z) + (D)4.5 * (ux * nx + uy * ny + uz * nz);
+    const D Bx = (D)3 * (m1x + (D)3 * nx - ux * L0);
+    const D By = (D)3 * (m1y + (D)3 * ny - uy * L0);
+    const D Bz = (D)3 * (m1z + (D)3 * nz - uz * L0);
+    const D G = A - (Bx * ux + By * uy + Bz * uz);
+    dw = (double)S2 * (double)rinv;
+    const R om1 = (R)1 - omega;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      const R lam = (R)__ldg(lin.p[q] + offp(q));
+      const R mu = om1 * lam + omega * (R)(G + cdot<D>(q, Bx, By, Bz));
+      lout.p[q][o] = (S)mu;
+    }
+  }
+  for (int sft = 16; sft > 0; sft >>= 1) dw += __shfl_down_sync(0xffffffffu, dw, sft);
+  const int t = threadIdx.x + blockDim.x * threadIdx.y;
+  if ((t & 31) == 0) wsum[t >> 5] = dw;
+  __syncthreads();
+  if (t == 0) {
+    double s = 0.0;
+    for (int w = 0; w < 4; ++w) s += wsum[w];
+    const long long b = blockIdx.x + (long long)gridDim.x * (blockIdx.y + (long long)gridDim.y * blockIdx.z);
+    KS a2{acc[2 * b], acc[2 * b + 1]};
+    kadd(a2, s);
+    acc[2 * b] = a2.s;
+    acc[2 * b + 1] = a2.c;
+  }
+}
+
 template <class F>
 __global__ void __launch_bounds__(DIAG_THREADS) k_adj_grad_u0(Pops<const typename F::S> lam, Geo g,
                                                               const double* __restrict__ u0, double* grad) {
@@ -373,6 +480,30 @@ cudaError_t launch_adj_step(const Lattice& ft, const Lattice& lin, const Lattice
                                                ft.g, omega, acc)),
       (k_adj_step<F32><<<grid, block, 0, st>>>(pops<const float>(ft), pops<const float>(lin), pops<float>(lout),
                                                ft.g, (float)omega, acc)))
+}
+
+cudaError_t launch_adj_inv(const Lattice& post, bool first, const Lattice& lin, const Lattice& lout,
+                           const Lattice* gout, double omega, double* acc, cudaStream_t st) {
+  dim3 grid, block;
+  adj_shape(post.g, &grid, &block);
+  const int sg = gout != nullptr;
+  const Lattice& go = gout ? *gout : lout;  // not written when sg = 0
+  const double rinv = 1.0 / (1.0 - omega);
+  switch (post.form) {
+    case FORM_F64: {
+      auto kf = first ? k_adj_inv<F64, true> : k_adj_inv<F64, false>;
+      kf<<<grid, block, 0, st>>>(pops<const double>(post), pops<const double>(lin), pops<double>(lout),
+                                 pops<double>(go), sg, post.g, omega, rinv, acc);
+      return cudaGetLastError();
+    }
+    case FORM_F32: {
+      auto kf = first ? k_adj_inv<F32, true> : k_adj_inv<F32, false>;
+      kf<<<grid, block, 0, st>>>(pops<const float>(post), pops<const float>(lin), pops<float>(lout),
+                                 pops<float>(go), sg, post.g, (float)omega, (float)rinv, acc);
+      return cudaGetLastError();
+    }
+  }
+  return cudaErrorInvalidValue;
 }
 
 cudaError_t launch_acc_total_n(const double* acc, long long n, double* total, cudaStream_t st) {

@@ -101,6 +101,7 @@ struct bgk_ctx {
   long long adj_acc_n = 0;
   double* adj_tot = nullptr;
   size_t adj_cache_bytes = 0;  // bgk_adjoint_cache budget
+  int adj_mode = BGK_ADJ_RECOMPUTE;  // bgk_adjoint_mode
   // z-slab (proc_z > 1): ghost buffer [parity 2][face 2][NZF][plane_elems],
   // the neighbours' buffers, and whether the neighbours' planes were filled
   // from the current state
@@ -1260,6 +1261,15 @@ struct AdjBufs {
   }
 };
 
+// The rebuilt states of a segment of K steps carry the rounding of up to K - 1
+// inverted collisions, each of which scales the non-equilibrium part by
+// 1 / |1 - omega|: rebuilding is used while |1 - omega|^-(K-1) <= 64.
+bool adj_rebuild_ok(double omega, int K) {
+  const double r = std::fabs(1.0 - omega);
+  if (!(r > 0.0) || K < 1) return false;
+  return (K - 1) * std::log(1.0 / r) <= std::log(64.0);
+}
+
 int adj_check(bgk_ctx* c, int nsteps) {
   int rc = check_ctx(c);
   if (rc) return rc;
@@ -1311,8 +1321,11 @@ int bgk_adjoint(bgk_ctx* c, const double* u0, const double* v0, const double* w0
   CK(cudaSetDevice(c->p.device));
   const int T = nsteps, K = ckpt_every < nsteps ? ckpt_every : nsteps;
   const int nck = (T + K - 1) / K;
-  const int nwork = K - 1 > 2 ? K - 1 : 2;
   const bool want_grad = grad_u0 || grad_tau;
+  // rebuild the states of a segment backwards from the state that ends it
+  // when the rounding of K - 1 rebuilt steps grows by at most 64x
+  const bool rebuild = want_grad && c->adj_mode == BGK_ADJ_REBUILD && adj_rebuild_ok(c->omega, K);
+  const int nwork = (K - 1 > 2 && !rebuild) ? K - 1 : 2;
   AdjBufs B(c);
   double *du0 = nullptr, *dut = nullptr, *acc = nullptr, *tot = nullptr;
   if ((rc = upload3(c, 0, u0, v0, w0, &du0, "initial velocity"))) return rc;
@@ -1371,6 +1384,21 @@ int bgk_adjoint(bgk_ctx* c, const double* u0, const double* v0, const double* w0
     int li = 0;  // lam[li] holds lam^{t+1}
     for (int s = nck - 1; s >= 0; --s) {
       const int t0 = s * K, t1 = t0 + K < T ? t0 + K : T;
+      if (s < s_cache && rebuild) {
+        // from f^{t1} (the next checkpoint, or the final state) down to t0:
+        // each launch rebuilds g^t into the work lattice it does not read
+        const Lattice* post = s == nck - 1 ? cur : &ck[s + 1];
+        int gi = post == &work[0] ? 1 : 0;
+        for (int t = t1 - 1; t >= t0; --t) {
+          const bool first = t == t1 - 1, last = t == t0;
+          CK(launch_adj_inv(*post, first, lam[li], lam[li ^ 1], last ? nullptr : &work[gi], c->omega, acc, c->st));
+          li ^= 1;
+          post = &work[gi];
+          gi ^= 1;
+        }
+        c->launches += t1 - t0;
+        continue;
+      }
       std::vector<const Lattice*> st(t1 - t0);
       st[0] = &ck[s];
       for (int m = 1; m < t1 - t0; ++m) {
@@ -1404,6 +1432,19 @@ int bgk_adjoint(bgk_ctx* c, const double* u0, const double* v0, const double* w0
   if (grad_tau) *grad_tau = -c->omega * c->omega * h[1];  // tau = 1/omega
   return BGK_OK;
 }
+
+int bgk_adjoint_mode(bgk_ctx* c, int mode) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (mode != BGK_ADJ_RECOMPUTE && mode != BGK_ADJ_REBUILD) {
+    set_err("bgk_adjoint_mode: mode must be BGK_ADJ_RECOMPUTE or BGK_ADJ_REBUILD");
+    return BGK_ERR_INVALID;
+  }
+  c->adj_mode = mode;
+  return BGK_OK;
+}
+
+int bgk_adjoint_rebuilds(double omega, int ckpt_every) { return adj_rebuild_ok(omega, ckpt_every) ? 1 : 0; }
 
 int bgk_adjoint_cache(bgk_ctx* c, size_t bytes) {
   int rc = check_ctx(c);

@@ -63,6 +63,14 @@ long long adj_step_blocks(const Geo& g);
 cudaError_t launch_acc_total_n(const double* acc, long long n, double* total, cudaStream_t st);
 cudaError_t launch_adj_step(const Lattice& ft, const Lattice& lam_in, const Lattice& lam_out, double omega,
                             double* acc, cudaStream_t st);
+// The same adjoint step on a state rebuilt from the one after it: post is the
+// state after the step, read unshifted (first: a stored forward state) or,
+// when first is false, the g that the previous launch rebuilt (gathered from
+// x + c_q); writes lam_out and, when gout is not null, the rebuilt
+// pre-collision g for the next launch. Same launch shape and acc pairs as
+// launch_adj_step.
+cudaError_t launch_adj_inv(const Lattice& post, bool first, const Lattice& lam_in, const Lattice& lam_out,
+                           const Lattice* gout, double omega, double* acc, cudaStream_t st);
 // dL/du0 (3 dense arrays) from lam at t = 0 and the initial velocity u0.
 cudaError_t launch_adj_grad_u0(const Lattice& lam0, const double* u0, double* grad, cudaStream_t st);
 // Tangent-linear model: perturbation of the initial state from du0 ...

@@ -245,6 +245,28 @@ int bgk_adjoint(bgk_ctx* ctx, const double* u0, const double* v0, const double* 
    other adjoint buffers; a smaller budget frees them. */
 int bgk_adjoint_cache(bgk_ctx* ctx, size_t bytes);
 
+/* How bgk_adjoint's backward pass obtains the forward states between
+   checkpoints (no reference counterpart).
+   BGK_ADJ_RECOMPUTE (default): runs the forward again from each checkpoint
+   and keeps the segment's states; the gradient is the exact discrete adjoint
+   of the stored trajectory.
+   BGK_ADJ_REBUILD: rebuilds them backwards from the state that ends each
+   segment, inside the adjoint step: the BGK collision keeps rho and j, so the
+   post-collision populations x of a cell give the pre-collision ones
+   g = (x - omega e(x)) / (1 - omega). No recomputation and no segment states
+   (2 work lattices instead of ckpt_every - 1): one backward step moves
+   4 x 19 populations per cell against 19 + 19 (recomputation) + 3 x 19
+   (adjoint step). The rebuilt states equal the forward's up to rounding,
+   which grows by up to 1/|1 - omega| per rebuilt step; the mode applies only
+   where |1 - omega|^-(ckpt_every - 1) <= 64 (bgk_adjoint_rebuilds), and
+   bgk_adjoint recomputes otherwise. Cached segments (bgk_adjoint_cache) use
+   their kept states in either mode. */
+#define BGK_ADJ_RECOMPUTE 0
+#define BGK_ADJ_REBUILD 1
+int bgk_adjoint_mode(bgk_ctx* ctx, int mode);
+/* 1 when BGK_ADJ_REBUILD applies to omega and ckpt_every, else 0. */
+int bgk_adjoint_rebuilds(double omega, int ckpt_every);
+
 /* Tangent-linear run (forward-mode derivative) of the same loss: dloss is the
    derivative of loss along the perturbation (du0, dv0, dw0) of the initial
    velocity and dtau of tau. Used to check bgk_adjoint:

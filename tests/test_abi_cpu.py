@@ -214,3 +214,24 @@ def test_bench_kernel_names_and_shared_config():
     a.decomp = "slabs"
     c4 = bench.config_of(a, 4)
     assert c4["box"] == [256, 256, 1024] and c4["slabs"] == 4
+
+
+def test_header_constants_match_the_binding(bgk):
+    txt = open(HEADER).read()
+    defs = {k: int(v) for k, v in re.findall(r"#define (BGK_\w+) \(?(-?\d+)\)?", txt)}
+    assert len(defs) >= 15
+    for k, v in defs.items():
+        assert getattr(bgk._abi, k) == v, k
+
+
+def test_adjoint_rebuild_rule(bgk):
+    """BGK_ADJ_REBUILD applies while |1 - omega|^-(K-1) <= 64: host-only query."""
+    lib = bgk.load()
+    assert lib.bgk_adjoint_rebuilds(1.0 / 0.51, 32) == 1   # 1.041^31 = 3.5
+    assert lib.bgk_adjoint_rebuilds(1.0 / 0.505, 200) == 1  # 1.02^199 = 52
+    assert lib.bgk_adjoint_rebuilds(1.0 / 0.505, 250) == 0
+    assert lib.bgk_adjoint_rebuilds(1.0 / 0.6, 32) == 0    # 1.5^31
+    assert lib.bgk_adjoint_rebuilds(1.0 / 0.6, 8) == 1     # 1.5^7 = 17
+    assert lib.bgk_adjoint_rebuilds(1.0, 2) == 0           # omega = 1: the collision forgets g
+    assert lib.bgk_adjoint_rebuilds(1.25, 1) == 1          # one step per segment: nothing rebuilt twice
+    assert lib.bgk_adjoint_rebuilds(1.9, 0) == 0

@@ -200,3 +200,82 @@ def test_adjoint_study_small_case(bgk):
     assert r["tangent"]["max_rel_err"] <= 1e-9, r["tangent"]
     assert r["fd"]["tau_rel_err"] <= 1e-5, r["fd"]
     assert r["loss"] == r["loss_in_adjoint_call"]
+
+
+def _set_mode(box, mode):
+    assert box._lib.bgk_adjoint_mode(box._h, mode) == 0, box._lib.bgk_last_error()
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_adjoint_rebuild_matches_recompute(bgk, precision):
+    """Rebuilding the forward states backwards (BGK_ADJ_REBUILD) gives the
+    recomputed gradient up to the rounding of the rebuilt states: the loss is
+    the same forward's, the gradients agree to 1e-11 (FP64) and 2e-5 (FP32)
+    relative, in rel. L2 for dL/du0."""
+    n, T, K = 16, 24, 6
+    u0, ut = fields(n, 1), fields(n, 2)
+    box = bgk.BGK3D(n, svisc=0.01, precision=precision)
+    assert box._lib.bgk_adjoint_rebuilds(box.omega, K) == 1
+    ref = adjoint(box, u0, ut, T, K)
+    _set_mode(box, bgk._abi.BGK_ADJ_REBUILD)
+    got = adjoint(box, u0, ut, T, K)
+    tol = 1e-11 if precision == "fp64" else 2e-5
+    assert got[0] == ref[0]
+    assert _rel(got[1], ref[1]) <= tol
+    assert got[2] == pytest.approx(ref[2], rel=tol)
+    # T not a multiple of K, K = 1 (every step a first and last one), K = T
+    for T2, K2 in ((23, 5), (7, 1), (9, 9)):
+        _set_mode(box, bgk._abi.BGK_ADJ_RECOMPUTE)
+        ref = adjoint(box, u0, ut, T2, K2)
+        _set_mode(box, bgk._abi.BGK_ADJ_REBUILD)
+        got = adjoint(box, u0, ut, T2, K2)
+        assert got[0] == ref[0]
+        assert _rel(got[1], ref[1]) <= tol, (T2, K2)
+        assert got[2] == pytest.approx(ref[2], rel=tol)
+    box.close()
+
+
+def test_adjoint_rebuild_matches_tangent_linear(bgk):
+    """Dot-product test of the rebuilt-state adjoint against the tangent
+    model along the stored forward trajectory, 1e-9 relative (FP64)."""
+    n, T = 16, 24
+    u0, ut = fields(n, 1), fields(n, 2)
+    box = bgk.BGK3D(n, svisc=0.01)
+    _set_mode(box, bgk._abi.BGK_ADJ_REBUILD)
+    loss, g, gtau = adjoint(box, u0, ut, T, 8)
+    du = np.random.default_rng(3).standard_normal((3, n, n, n))
+    dtau = 0.7
+    _, dl = tangent(box, u0, du, dtau, ut, T)
+    assert float(np.dot(g, du.reshape(-1))) + gtau * dtau == pytest.approx(dl, rel=1e-9)
+    box.close()
+
+
+def test_adjoint_rebuild_with_state_cache_and_rule(bgk):
+    """Cached segments use their kept states and the others are rebuilt; where
+    |1 - omega|^-(K-1) > 64 (omega = 1.25, K = 6) the call recomputes, and
+    then its results equal the recompute mode's bit for bit."""
+    n, T, K = 12, 17, 4
+    u0, ut = fields(n, 4), fields(n, 5)
+    box = bgk.BGK3D(n, svisc=0.02)
+    lib = box._lib
+    ref = adjoint(box, u0, ut, T, K)
+    _set_mode(box, bgk._abi.BGK_ADJ_REBUILD)
+    state = 19 * 32 * n * n * 8
+    assert lib.bgk_adjoint_cache(box._h, 2 * state * (K - 1)) == 0
+    got = adjoint(box, u0, ut, T, K)
+    assert got[0] == ref[0] and _rel(got[1], ref[1]) <= 1e-11
+    assert lib.bgk_adjoint_cache(box._h, 0) == 0
+    box.close()
+    box = bgk.BGK3D(n, omega=1.25)
+    lib = box._lib
+    assert lib.bgk_adjoint_rebuilds(1.25, 6) == 0 and lib.bgk_adjoint_rebuilds(1.25, 3) == 1
+    ref = adjoint(box, u0, ut, T, 6)
+    _set_mode(box, bgk._abi.BGK_ADJ_REBUILD)
+    got = adjoint(box, u0, ut, T, 6)
+    assert got[0] == ref[0] and got[2] == ref[2] and np.array_equal(got[1], ref[1])
+    assert lib.bgk_adjoint_mode(box._h, 7) == bgk._abi.BGK_ERR_INVALID
+    box.close()

@@ -23,7 +23,8 @@ boundaries + col_MC). Prints one JSON line.
   initial velocity field uploaded from pinned host memory, then
   boundaries + col_MC + diagnostic every step (diagnostics computed every
   icheck = 100 steps, the reference's default, SRC/input.F90:221, and read
-  back to the host), all inside the timed region; split into the one-time
+  back to the host), all inside the timed region, after an untimed warm-up
+  pass of the same calls (upload, init and W steps); split into the one-time
   part (upload + init, fixed_ms) and the per-step part (per_step_ms).
 - roofline: algorithmic bytes of the stream-collide kernel (19 loads + 19
   stores per cell) per launch / average launch time, against the measured HBM
@@ -431,6 +432,14 @@ def run_ours(a):
         box2 = B.BGK3D(L, svisc=svisc, u0=0.03, precision=a.precision, scheme=a.scheme, icheck=a.icheck,
                        device=local, kernel=a.kernel, les_cs=a.les_cs)
         stream2 = torch.cuda.ExternalStream(box2.stream, device=local)
+        # warm-up pass of the same calls (upload, init, W steps), untimed: the
+        # context's upload staging and the first-use costs of the pinned pages
+        # stay out of the timed pass, which uploads and initialises again
+        box2.init_velocity(*(p.numpy() for p in pin))
+        for it in range(1, a.warmup + 1):
+            box2.boundaries(it)
+            box2.col_MC(it)
+        box2.synchronize()
         torch.cuda.synchronize()
         if ws > 1:
             torch.distributed.barrier()

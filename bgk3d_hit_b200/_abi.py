@@ -82,7 +82,7 @@ PROTOTYPES = [
     ("bgk_adjoint", _i, [_vp, _dp, _dp, _dp, _dp, _dp, _dp, _i, _i, _dp, _dp, _dp]),
     ("bgk_adjoint_cache", _i, [_vp, C.c_size_t]),
     ("bgk_adjoint_mode", _i, [_vp, _i]),
-    ("bgk_adjoint_rebuilds", _i, [_d, _i]),
+    ("bgk_adjoint_rebuilds", _i, [_i, _d, _i]),
     ("bgk_tangent", _i, [_vp, _dp, _dp, _dp, _dp, _dp, _dp, _d, _dp, _dp, _dp, _i, _dp, _dp]),
     ("bgk_get_scale", _i, [_vp, _dp]),
     ("bgk_get_omega", _i, [_vp, _dp]),

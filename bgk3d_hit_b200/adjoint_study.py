@@ -70,7 +70,7 @@ def run(size=128, steps=1000, ckpt=32, tau=0.51, k0=4.0, u_rms=0.03, dirs=64, h=
     if cache_gb > 0:
         box._lib.bgk_adjoint_cache(box._h, int(cache_gb * 1e9))
     if mode == "rebuild":
-        if not box._lib.bgk_adjoint_rebuilds(box.omega, ckpt):
+        if not box._lib.bgk_adjoint_rebuilds(_abi.PRECISIONS[precision], box.omega, ckpt):
             raise ValueError("rebuild mode does not apply to tau %g with a checkpoint every %d steps" % (tau, ckpt))
         box._lib.bgk_adjoint_mode(box._h, _abi.BGK_ADJ_REBUILD)
     tau_used = 1.0 / box.omega

@@ -1263,11 +1263,17 @@ struct AdjBufs {
 
 // The rebuilt states of a segment of K steps carry the rounding of up to K - 1
 // inverted collisions, each of which scales the non-equilibrium part by
-// 1 / |1 - omega|: rebuilding is used while |1 - omega|^-(K-1) <= 64.
-bool adj_rebuild_ok(double omega, int K) {
+// 1 / |1 - omega|, so their relative error grows to about
+// K * A * (the form's rounding), A = |1 - omega|^-(K-1). Rebuilding is used
+// while A <= 64 and, in FP32 storage (rounding 6e-8), K * A <= 160: a
+// rebuilt-state error below about 1e-5, under the 4.5e-5 between the FP32
+// and FP64 gradients (FP64: below 1e-12).
+bool adj_rebuild_ok(int form, double omega, int K) {
   const double r = std::fabs(1.0 - omega);
-  if (!(r > 0.0) || K < 1) return false;
-  return (K - 1) * std::log(1.0 / r) <= std::log(64.0);
+  if (!(r > 0.0) || K < 1 || (form != FORM_F64 && form != FORM_F32)) return false;
+  const double logA = (K - 1) * std::log(1.0 / r);
+  if (logA > std::log(64.0)) return false;
+  return form == FORM_F64 || std::log((double)K) + logA <= std::log(160.0);
 }
 
 int adj_check(bgk_ctx* c, int nsteps) {
@@ -1324,7 +1330,7 @@ int bgk_adjoint(bgk_ctx* c, const double* u0, const double* v0, const double* w0
   const bool want_grad = grad_u0 || grad_tau;
   // rebuild the states of a segment backwards from the state that ends it
   // when the rounding of K - 1 rebuilt steps grows by at most 64x
-  const bool rebuild = want_grad && c->adj_mode == BGK_ADJ_REBUILD && adj_rebuild_ok(c->omega, K);
+  const bool rebuild = want_grad && c->adj_mode == BGK_ADJ_REBUILD && adj_rebuild_ok(c->form, c->omega, K);
   const int nwork = (K - 1 > 2 && !rebuild) ? K - 1 : 2;
   AdjBufs B(c);
   double *du0 = nullptr, *dut = nullptr, *acc = nullptr, *tot = nullptr;
@@ -1444,7 +1450,10 @@ int bgk_adjoint_mode(bgk_ctx* c, int mode) {
   return BGK_OK;
 }
 
-int bgk_adjoint_rebuilds(double omega, int ckpt_every) { return adj_rebuild_ok(omega, ckpt_every) ? 1 : 0; }
+int bgk_adjoint_rebuilds(int precision, double omega, int ckpt_every) {
+  const int form = precision == BGK_FP64 ? FORM_F64 : precision == BGK_FP32DEV ? FORM_F32 : -1;
+  return adj_rebuild_ok(form, omega, ckpt_every) ? 1 : 0;
+}
 
 int bgk_adjoint_cache(bgk_ctx* c, size_t bytes) {
   int rc = check_ctx(c);

@@ -257,15 +257,17 @@ int bgk_adjoint_cache(bgk_ctx* ctx, size_t bytes);
    (2 work lattices instead of ckpt_every - 1): one backward step moves
    4 x 19 populations per cell against 19 + 19 (recomputation) + 3 x 19
    (adjoint step). The rebuilt states equal the forward's up to rounding,
-   which grows by up to 1/|1 - omega| per rebuilt step; the mode applies only
-   where |1 - omega|^-(ckpt_every - 1) <= 64 (bgk_adjoint_rebuilds), and
+   which grows by up to 1/|1 - omega| per rebuilt step: with
+   A = |1 - omega|^-(ckpt_every - 1), the mode applies where A <= 64 and, in
+   the FP32 form, ckpt_every * A <= 160 (bgk_adjoint_rebuilds), and
    bgk_adjoint recomputes otherwise. Cached segments (bgk_adjoint_cache) use
    their kept states in either mode. */
 #define BGK_ADJ_RECOMPUTE 0
 #define BGK_ADJ_REBUILD 1
 int bgk_adjoint_mode(bgk_ctx* ctx, int mode);
-/* 1 when BGK_ADJ_REBUILD applies to omega and ckpt_every, else 0. */
-int bgk_adjoint_rebuilds(double omega, int ckpt_every);
+/* 1 when BGK_ADJ_REBUILD applies to the form `precision` (BGK_FP64 or
+   BGK_FP32DEV), omega and ckpt_every, else 0. */
+int bgk_adjoint_rebuilds(int precision, double omega, int ckpt_every);
 
 /* Tangent-linear run (forward-mode derivative) of the same loss: dloss is the
    derivative of loss along the perturbation (du0, dv0, dw0) of the initial

@@ -225,13 +225,20 @@ def test_header_constants_match_the_binding(bgk):
 
 
 def test_adjoint_rebuild_rule(bgk):
-    """BGK_ADJ_REBUILD applies while |1 - omega|^-(K-1) <= 64: host-only query."""
+    """BGK_ADJ_REBUILD applies while A = |1 - omega|^-(K-1) <= 64 and, in the
+    FP32 form, K * A <= 160: host-only query."""
     lib = bgk.load()
-    assert lib.bgk_adjoint_rebuilds(1.0 / 0.51, 32) == 1   # 1.041^31 = 3.5
-    assert lib.bgk_adjoint_rebuilds(1.0 / 0.505, 200) == 1  # 1.02^199 = 52
-    assert lib.bgk_adjoint_rebuilds(1.0 / 0.505, 250) == 0
-    assert lib.bgk_adjoint_rebuilds(1.0 / 0.6, 32) == 0    # 1.5^31
-    assert lib.bgk_adjoint_rebuilds(1.0 / 0.6, 8) == 1     # 1.5^7 = 17
-    assert lib.bgk_adjoint_rebuilds(1.0, 2) == 0           # omega = 1: the collision forgets g
-    assert lib.bgk_adjoint_rebuilds(1.25, 1) == 1          # one step per segment: nothing rebuilt twice
-    assert lib.bgk_adjoint_rebuilds(1.9, 0) == 0
+    F64, F32, F16 = bgk._abi.BGK_FP64, bgk._abi.BGK_FP32DEV, bgk._abi.BGK_FP16DEV
+    for f in (F64, F32):
+        assert lib.bgk_adjoint_rebuilds(f, 1.0 / 0.51, 32) == 1  # A = 1.041^31 = 3.5, K A = 111
+        assert lib.bgk_adjoint_rebuilds(f, 1.0 / 0.6, 32) == 0  # A = 1.5^31
+        assert lib.bgk_adjoint_rebuilds(f, 1.0 / 0.6, 8) == 1  # A = 1.5^7 = 17, K A = 137
+        assert lib.bgk_adjoint_rebuilds(f, 1.0, 2) == 0  # omega = 1: the collision forgets g
+        assert lib.bgk_adjoint_rebuilds(f, 1.25, 1) == 1  # one step per segment: nothing rebuilt twice
+        assert lib.bgk_adjoint_rebuilds(f, 1.9, 0) == 0
+    assert lib.bgk_adjoint_rebuilds(F64, 1.0 / 0.505, 200) == 1  # A = 1.02^199 = 52
+    assert lib.bgk_adjoint_rebuilds(F64, 1.0 / 0.505, 250) == 0  # A = 145
+    assert lib.bgk_adjoint_rebuilds(F32, 1.0 / 0.505, 200) == 0  # K A = 10400
+    assert lib.bgk_adjoint_rebuilds(F32, 1.0 / 0.505, 60) == 0  # A = 3.3, K A = 195
+    assert lib.bgk_adjoint_rebuilds(F32, 1.0 / 0.505, 50) == 1  # A = 2.7, K A = 133
+    assert lib.bgk_adjoint_rebuilds(F16, 1.0 / 0.51, 32) == 0  # no adjoint in FP16

@@ -219,7 +219,7 @@ def test_adjoint_rebuild_matches_recompute(bgk, precision):
     n, T, K = 16, 24, 6
     u0, ut = fields(n, 1), fields(n, 2)
     box = bgk.BGK3D(n, svisc=0.01, precision=precision)
-    assert box._lib.bgk_adjoint_rebuilds(box.omega, K) == 1
+    assert box._lib.bgk_adjoint_rebuilds(bgk._abi.PRECISIONS[precision], box.omega, K) == 1
     ref = adjoint(box, u0, ut, T, K)
     _set_mode(box, bgk._abi.BGK_ADJ_REBUILD)
     got = adjoint(box, u0, ut, T, K)
@@ -272,7 +272,7 @@ def test_adjoint_rebuild_with_state_cache_and_rule(bgk):
     box.close()
     box = bgk.BGK3D(n, omega=1.25)
     lib = box._lib
-    assert lib.bgk_adjoint_rebuilds(1.25, 6) == 0 and lib.bgk_adjoint_rebuilds(1.25, 3) == 1
+    assert lib.bgk_adjoint_rebuilds(0, 1.25, 6) == 0 and lib.bgk_adjoint_rebuilds(0, 1.25, 3) == 1
     ref = adjoint(box, u0, ut, T, 6)
     _set_mode(box, bgk._abi.BGK_ADJ_REBUILD)
     got = adjoint(box, u0, ut, T, 6)

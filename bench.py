@@ -192,6 +192,10 @@ def kernel_key(precision, scheme, L, kernel=0, les=False):
         if L % 2 == 0 and tpr & (tpr - 1) == 0 and (L * tpr) % 32 == 0:
             return ("k_two_f32v" if scheme == "two_lattice" else "k_aa_f32v") + ("_les" if les else "")
     allowed = (0, 4) if (les or scheme == "aa") else (0, 2, 4)  # the LES collision runs on four cells only
+    if precision == "fp16" and scheme == "aa" and not les and kernel == 0:
+        tpr = L // 8  # the odd step on eight cells per thread, the even one on four
+        if L % 8 == 0 and tpr & (tpr - 1) == 0 and (L * tpr) % 32 == 0:
+            return "k_aa_f16w"
     if precision == "fp16" and kernel in allowed:
         v = 2 if kernel == 2 else 4
         tpr = L // v

@@ -9,6 +9,8 @@
 //                the same updates with two FP32 / four FP16 cells of a row per
 //                thread (8-byte accesses, x-crossing values by warp shuffle);
 //                the defaults of those forms where a box fits them
+//   k_aa_f16w    the FP16 AA odd step with eight cells per thread (16-byte
+//                accesses), its default where a box fits it
 //   k_slab       two-lattice step of one z-slab with the face exchange fused in
 //   k_init_*     equilibrium initial conditions (SRC/init.F90:83-141)
 //   k_diag       diagno + dissipation + strain-rate sums (SRC/diagno.F90:73-121,
@@ -576,6 +578,175 @@ __global__ void __launch_bounds__(128, 5) k_aa_f16v(Pops<__half> a, Geo g, StepK
       const unsigned fp = cxq(q) > 0 && xl.edge_prev && prev_in ? xs_last[wprev][q] : 0u;
       const unsigned fn = cxq(q) < 0 && xl.edge_next && next_in ? xs_first[wnext][q - 9] : 0u;
       shift_out(Y[q], cxq(q), a.p[q] + row_out(cyq(q), czq(q)), i0, i_prev, i_next, xl, prev_in, next_in, fp, fn);
+    }
+  }
+}
+
+// FP16 AA pattern with eight cells per thread: k_aa_f16v's structure on
+// 16-byte chunks (cells i0..i0+7, i0 = 8 pos, tpr = nx/8 threads per row), so
+// the per-thread work of the odd step's x-crossing (shuffles, warp-edge
+// values, the 18 shifted rows' addresses) is spread over twice the cells.
+// Per-cell arithmetic is collide4_f16's on each half of the chunk, so the
+// results are k_aa_f16v's. The odd instantiation is launched (128
+// registers, 4 blocks/SM); the even one measured no faster than k_aa_f16v.
+__device__ __forceinline__ void shift_rows8(uint4 (&Y)[Q], const unsigned short (&E)[Q], const XLanes& xl) {
+#pragma unroll
+  for (int q = 0; q < Q; ++q) {
+    const uint4 A = Y[q];
+    if (cxq(q) > 0) {  // elements i0-1 .. i0+6
+      unsigned prev = __shfl_sync(0xffffffffu, A.w >> 16, xl.src_prev);
+      if (xl.edge_prev) prev = E[q];
+      Y[q].x = __byte_perm(A.x, prev, 0x1054);
+      Y[q].y = __byte_perm(A.x, A.y, 0x5432);
+      Y[q].z = __byte_perm(A.y, A.z, 0x5432);
+      Y[q].w = __byte_perm(A.z, A.w, 0x5432);
+    } else if (cxq(q) < 0) {  // elements i0+1 .. i0+8
+      unsigned next = __shfl_sync(0xffffffffu, A.x & 0xffffu, xl.src_next);
+      if (xl.edge_next) next = E[q];
+      Y[q].x = __byte_perm(A.x, A.y, 0x5432);
+      Y[q].y = __byte_perm(A.y, A.z, 0x5432);
+      Y[q].z = __byte_perm(A.z, A.w, 0x5432);
+      Y[q].w = __byte_perm(A.w, next, 0x5432);
+    }
+  }
+}
+
+// Store side of the eight-cells odd step (shift_out on 16-byte chunks): cell
+// i0+m goes to element i0+m+cx; the aligned chunk i0..i0+7 is completed with
+// the neighbouring lane's crossing value, and at block boundaries the edge
+// lanes store their part with 2-, 4- and 8-byte stores.
+__device__ __forceinline__ void shift_out8(uint4 Y, int cx, __half* p, int i0, int i_prev, int i_next,
+                                           const XLanes& xl, bool prev_in, bool next_in, unsigned from_prev,
+                                           unsigned from_next) {
+  unsigned short* u = reinterpret_cast<unsigned short*>(p);
+  if (cx == 0) {
+    *reinterpret_cast<uint4*>(p + i0) = Y;
+  } else if (cx > 0) {  // cell i0+m -> element i0+m+1
+    unsigned prev = __shfl_sync(0xffffffffu, Y.w >> 16, xl.src_prev);  // cell i0-1 of the lane before
+    if (xl.edge_prev && prev_in) prev = from_prev;
+    const uint4 c = make_uint4(__byte_perm(prev, Y.x, 0x5410), __byte_perm(Y.x, Y.y, 0x5432),
+                               __byte_perm(Y.y, Y.z, 0x5432), __byte_perm(Y.z, Y.w, 0x5432));
+    if (!xl.edge_prev || prev_in) {
+      *reinterpret_cast<uint4*>(p + i0) = c;
+    } else {
+      u[i0 + 1] = (unsigned short)(Y.x & 0xffffu);
+      *reinterpret_cast<unsigned*>(p + i0 + 2) = c.y;
+      *reinterpret_cast<uint2*>(p + i0 + 4) = make_uint2(c.z, c.w);
+    }
+    if (xl.edge_next && !next_in) u[i_next] = (unsigned short)(Y.w >> 16);
+  } else {  // cell i0+m -> element i0+m-1
+    unsigned next = __shfl_sync(0xffffffffu, Y.x & 0xffffu, xl.src_next);  // cell i0+8 of the lane after
+    if (xl.edge_next && next_in) next = from_next;
+    const uint4 c = make_uint4(__byte_perm(Y.x, Y.y, 0x5432), __byte_perm(Y.y, Y.z, 0x5432),
+                               __byte_perm(Y.z, Y.w, 0x5432), __byte_perm(Y.w, next, 0x5432));
+    if (!xl.edge_next || next_in) {
+      *reinterpret_cast<uint4*>(p + i0) = c;
+    } else {
+      *reinterpret_cast<uint2*>(p + i0) = make_uint2(c.x, c.y);
+      *reinterpret_cast<unsigned*>(p + i0 + 4) = c.z;
+      u[i0 + 6] = (unsigned short)(Y.w >> 16);
+    }
+    if (xl.edge_prev && !prev_in) u[i_prev] = (unsigned short)(Y.x & 0xffffu);
+  }
+}
+
+template <bool ODD>
+__global__ void __launch_bounds__(128, 4) k_aa_f16w(Pops<__half> a, Geo g, StepK K, int log_tpr) {
+  const int tpr = 1 << log_tpr;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j0 = t >> log_tpr, pos = t & (tpr - 1);
+  const int k = blockIdx.y;
+  const bool valid = j0 < g.ny;  // whole warps: ny*tpr is a multiple of 32
+  if (!ODD && !valid) return;
+  const int j = valid ? j0 : 0;  // an idle warp of the odd step only reaches its barrier
+  const XLanes xl(tpr, pos, threadIdx.x & 31);
+  const int i0 = pos * 8;
+  const int jm = j == 0 ? g.ny - 1 : j - 1, jp = j == g.ny - 1 ? 0 : j + 1;
+  const int km = k == 0 ? g.nz - 1 : k - 1, kp = k == g.nz - 1 ? 0 : k + 1;
+  const int i_prev = pos == 0 ? g.nx - 1 : i0 - 1;
+  const int i_next = pos == tpr - 1 ? 0 : i0 + 8;
+  auto row = [&](int dy, int dz) {
+    const int jj = dy > 0 ? jp : (dy < 0 ? jm : j);
+    const int kk = dz > 0 ? kp : (dz < 0 ? km : k);
+    return g.sx * (jj + g.ny * kk);
+  };
+  uint4 Y[Q];
+  if (ODD && !valid) {
+#pragma unroll
+    for (int q = 0; q < Q; ++q) Y[q] = make_uint4(0u, 0u, 0u, 0u);
+  } else if (ODD) {
+    unsigned short E[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      const __half* p = a.p[oppq(q)] + row(-cyq(q), -czq(q));
+      Y[q] = __ldg(reinterpret_cast<const uint4*>(p + i0));
+      E[q] = 0;
+      if (cxq(q) > 0 && xl.edge_prev) E[q] = ldg_u16(p + i_prev);
+      if (cxq(q) < 0 && xl.edge_next) E[q] = ldg_u16(p + i_next);
+    }
+    shift_rows8(Y, E, xl);
+  } else {
+#pragma unroll
+    for (int q = 0; q < Q; ++q) Y[q] = __ldg(reinterpret_cast<const uint4*>(a.p[q] + row(0, 0) + i0));
+  }
+  if (valid) {
+    uint2 L[Q], H[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      L[q] = make_uint2(Y[q].x, Y[q].y);
+      H[q] = make_uint2(Y[q].z, Y[q].w);
+    }
+    collide4_f16<false>(L, K);
+    collide4_f16<false>(H, K);
+#pragma unroll
+    for (int q = 0; q < Q; ++q) Y[q] = make_uint4(L[q].x, L[q].y, H[q].x, H[q].y);
+  }
+  __shared__ unsigned xs_last[ODD ? 4 : 1][5], xs_first[ODD ? 4 : 1][5];
+  bool prev_in = false, next_in = false;
+  int wprev = 0, wnext = 0;
+  if (ODD) {
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (tpr >= 32) {
+      const int nw = tpr >> 5, r = pos >> 5;
+      if (nw <= 4) {
+        prev_in = next_in = true;
+        wprev = w - r + (r + nw - 1) % nw;
+        wnext = w - r + (r + 1) % nw;
+      } else {
+        prev_in = w > 0;
+        next_in = w < 3;
+        wprev = w - 1;
+        wnext = w + 1;
+      }
+      if (valid && lane == 31) {
+#pragma unroll
+        for (int q = 0; q < 5; ++q) xs_last[w][q] = Y[q].w >> 16;
+      }
+      if (valid && lane == 0) {
+#pragma unroll
+        for (int q = 9; q < 14; ++q) xs_first[w][q - 9] = Y[q].x & 0xffffu;
+      }
+    }
+    __syncthreads();
+    if (!valid) return;
+  }
+  int js = j, ks = k;
+  if (ODD) asm volatile("" : "+r"(js), "+r"(ks));
+  const int jms = js == 0 ? g.ny - 1 : js - 1, jps = js == g.ny - 1 ? 0 : js + 1;
+  const int kms = ks == 0 ? g.nz - 1 : ks - 1, kps = ks == g.nz - 1 ? 0 : ks + 1;
+  auto row_out = [&](int dy, int dz) {
+    const int jj = dy > 0 ? jps : (dy < 0 ? jms : js);
+    const int kk = dz > 0 ? kps : (dz < 0 ? kms : ks);
+    return g.sx * (jj + g.ny * kk);
+  };
+#pragma unroll
+  for (int q = 0; q < Q; ++q) {
+    if (!ODD) {
+      *reinterpret_cast<uint4*>(a.p[oppq(q)] + row(0, 0) + i0) = Y[q];
+    } else {
+      const unsigned fp = cxq(q) > 0 && xl.edge_prev && prev_in ? xs_last[wprev][q] : 0u;
+      const unsigned fn = cxq(q) < 0 && xl.edge_next && next_in ? xs_first[wnext][q - 9] : 0u;
+      shift_out8(Y[q], cxq(q), a.p[q] + row_out(cyq(q), czq(q)), i0, i_prev, i_next, xl, prev_in, next_in, fp, fn);
     }
   }
 }
@@ -1376,6 +1547,16 @@ static cudaError_t aa_impl(const Lattice& a, int odd, const StepK& K, int varian
     bool launched = false;
     cudaError_t e = launch_rows(a, a, odd ? ROW_AA_ODD : ROW_AA_EVEN, K, st, &launched);
     if (e != cudaSuccess || launched) return e;
+  }
+  // FP16 odd step (automatic): eight cells per thread where the box fits it.
+  // On B200 the pair of AA steps measured 84.3 GLUPS at 256^3 and 86.0 at
+  // 512^3 against 80.0 and 81.6 with four cells per thread on both steps;
+  // eight cells on the even step as well measured the same (84.1, 86.1), so
+  // the even step stays on k_aa_f16v (96 registers, 5 blocks/SM)
+  const int lt8 = F::id == FORM_F16 && variant == 0 && odd ? vec_log_tpr(a.g, 8) : -1;
+  if (lt8 >= 0) {
+    k_aa_f16w<true><<<vec_grid(a.g, lt8, a.g.nz), 128, 0, st>>>(pops_of<__half>(a), a.g, K, lt8);
+    return cudaGetLastError();
   }
   // FP16: four cells per thread where the box fits it (automatic or 4)
   if (lt4 >= 0) {

@@ -90,7 +90,9 @@ typedef struct {
   double omega;        /* collision frequency override (e.g. 0 = pure streaming) */
   int extras;          /* 1: bgk_diagnostic also computes enstrophy */
   int kernel;          /* stream-collide kernel: 0 automatic (FP16: 4 where the box
-                          fits, FP32: 2 where it fits, else 1), 1 one cell per thread,
+                          fits, and 8 cells per thread for the BGK odd step of the AA
+                          scheme where the box fits that; FP32: 2 where it fits, else
+                          1), 1 one cell per thread,
                           2 two cells per thread (FP32 both schemes, FP16 two-lattice),
                           4 four cells per thread (FP16), 8 row pipeline with TMA bulk
                           copies into shared memory (rows up to about 5 KB); boxes a

@@ -197,7 +197,9 @@ def test_bench_kernel_names_and_shared_config():
     assert bench.kernel_key("fp64", "two_lattice", 256) == "k_two_fp64"
     assert bench.kernel_key("fp16", "two_lattice", 256) == "k_two_f16v"
     assert bench.kernel_key("fp16", "two_lattice", 256, kernel=2) == "k_two_f16v2"
-    assert bench.kernel_key("fp16", "aa", 1024) == "k_aa_f16v"
+    assert bench.kernel_key("fp16", "aa", 1024) == "k_aa_f16w"  # odd step on eight cells per thread
+    assert bench.kernel_key("fp16", "aa", 1024, kernel=4) == "k_aa_f16v"
+    assert bench.kernel_key("fp16", "aa", 12) == "k_aa_fp16"  # neither 8 nor 4 cells fit a row of 12
     assert bench.kernel_key("fp16", "two_lattice", 256, les=True) == "k_two_f16v_les"
     assert bench.kernel_key("fp16", "aa", 256, les=True) == "k_aa_f16v_les"
     assert bench.kernel_key("fp16", "two_lattice", 256, kernel=1) == "k_two_fp16"

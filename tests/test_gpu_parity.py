@@ -134,6 +134,24 @@ def test_fp16_aa_kernel_variants_bitexact(bgk, oracle_mod, kernel, shape):
     box.close()
 
 
+@pytest.mark.parametrize("shape", [(64, 32, 5), (256, 8, 6), (1024, 4, 3), (2048, 2, 3), (16, 64, 3),
+                                   (8, 128, 3), (128, 16, 8)])
+def test_fp16_aa_eight_cells_odd_step_bitexact(bgk, oracle_mod, shape):
+    """The automatic FP16 AA odd step with eight cells per thread (16-byte
+    chunks; rows of one lane, inside a warp, one warp, four warps in one block,
+    and eight warps over two blocks, whose block-boundary lanes store partial
+    chunks) gives the oracle's bits over steps of both parities, as does the
+    four-cells kernel it replaces (kernel = 4)."""
+    for kernel in (0, 4):
+        orc, box = make_pair(bgk, oracle_mod, shape, "fp16", scheme="aa", kernel=kernel)
+        for it in range(1, 6):
+            orc.step(0.01, periodic=True)
+            box.col_MC(it)
+            if it in (1, 2, 5):
+                assert same_bits(box.populations(), orc.get_pops()), f"kernel {kernel}, after {it} steps"
+        box.close()
+
+
 @pytest.mark.parametrize("form", ["fp64", "fp32", "fp16"])
 @pytest.mark.parametrize("scheme", ["two_lattice", "aa"])
 @pytest.mark.parametrize("shape", [(5, 7, 9), (64, 16, 8), (33, 20, 7), (256, 3, 2)])

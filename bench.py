@@ -187,6 +187,10 @@ def kernel_key(precision, scheme, L, kernel=0, les=False):
     """Name of the stream-collide kernel a launch runs (the key of
     profiles/ncu_traffic.json)."""
     kern = f"{'k_two' if scheme == 'two_lattice' else 'k_aa'}_{precision}" + ("_les" if les else "")
+    if precision == "fp32" and scheme == "aa" and kernel == 0:
+        tpr = L // 4  # the odd step on four cells per thread, the even one on two
+        if L % 4 == 0 and tpr & (tpr - 1) == 0 and (L * tpr) % 32 == 0:
+            return "k_aa_f32w" + ("_les" if les else "")
     if precision == "fp32" and kernel in (0, 2):  # two cells per thread, both schemes, BGK and LES
         tpr = L // 2
         if L % 2 == 0 and tpr & (tpr - 1) == 0 and (L * tpr) % 32 == 0:

@@ -9,8 +9,10 @@
 //                the same updates with two FP32 / four FP16 cells of a row per
 //                thread (8-byte accesses, x-crossing values by warp shuffle);
 //                the defaults of those forms where a box fits them
-//   k_aa_f16w    the FP16 AA odd step with eight cells per thread (16-byte
-//                accesses), its default where a box fits it
+//   k_aa_f16w, k_aa_f32w
+//                the AA odd step with eight FP16 (BGK) / four FP32 (BGK and
+//                Smagorinsky) cells per thread, 16-byte accesses: its default
+//                where a box fits it
 //   k_slab       two-lattice step of one z-slab with the face exchange fused in
 //   k_init_*     equilibrium initial conditions (SRC/init.F90:83-141)
 //   k_diag       diagno + dissipation + strain-rate sums (SRC/diagno.F90:73-121,
@@ -884,6 +886,144 @@ __global__ void __launch_bounds__(128, 5) k_aa_f32v(Pops<float> a, Geo g, StepK 
   }
 }
 
+// FP32 AA odd step with four cells per thread: k_aa_f32v's odd step on
+// 16-byte chunks of four floats (cells i0..i0+3, i0 = 4 pos, tpr = nx/4), so
+// its per-thread x-crossing work covers twice the cells, as k_aa_f16w does
+// for FP16. F32::cell's arithmetic on each cell: the results of k_aa<F32>.
+// 125 registers (127 with the Smagorinsky collision), 4 blocks/SM, no spills.
+__device__ __forceinline__ void shift_out4_f32(float4 Y, int cx, float* p, int i0, int i_prev, int i_next,
+                                               const XLanes& xl, bool prev_in, bool next_in, float from_prev,
+                                               float from_next) {
+  if (cx == 0) {
+    *reinterpret_cast<float4*>(p + i0) = Y;
+  } else if (cx > 0) {  // cell i0+m -> element i0+m+1
+    float prev = __shfl_sync(0xffffffffu, Y.w, xl.src_prev);  // cell i0-1 of the lane before
+    if (xl.edge_prev && prev_in) prev = from_prev;
+    if (!xl.edge_prev || prev_in) {
+      *reinterpret_cast<float4*>(p + i0) = make_float4(prev, Y.x, Y.y, Y.z);
+    } else {
+      p[i0 + 1] = Y.x;
+      *reinterpret_cast<float2*>(p + i0 + 2) = make_float2(Y.y, Y.z);
+    }
+    if (xl.edge_next && !next_in) p[i_next] = Y.w;
+  } else {  // cell i0+m -> element i0+m-1
+    float next = __shfl_sync(0xffffffffu, Y.x, xl.src_next);  // cell i0+4 of the lane after
+    if (xl.edge_next && next_in) next = from_next;
+    if (!xl.edge_next || next_in) {
+      *reinterpret_cast<float4*>(p + i0) = make_float4(Y.y, Y.z, Y.w, next);
+    } else {
+      *reinterpret_cast<float2*>(p + i0) = make_float2(Y.y, Y.z);
+      p[i0 + 2] = Y.w;
+    }
+    if (xl.edge_prev && !prev_in) p[i_prev] = Y.x;
+  }
+}
+
+template <bool LES = false>
+__global__ void __launch_bounds__(128, 4) k_aa_f32w(Pops<float> a, Geo g, StepK K, int log_tpr) {
+  const int tpr = 1 << log_tpr;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j0 = t >> log_tpr, pos = t & (tpr - 1);
+  const int k = blockIdx.y;
+  const bool valid = j0 < g.ny;  // whole warps: ny*tpr is a multiple of 32
+  const int j = valid ? j0 : 0;  // an idle warp only reaches its barrier
+  const XLanes xl(tpr, pos, threadIdx.x & 31);
+  const int i0 = pos * 4;
+  const int jm = j == 0 ? g.ny - 1 : j - 1, jp = j == g.ny - 1 ? 0 : j + 1;
+  const int km = k == 0 ? g.nz - 1 : k - 1, kp = k == g.nz - 1 ? 0 : k + 1;
+  const int i_prev = pos == 0 ? g.nx - 1 : i0 - 1;
+  const int i_next = pos == tpr - 1 ? 0 : i0 + 4;
+  auto row = [&](int dy, int dz) {
+    const int jj = dy > 0 ? jp : (dy < 0 ? jm : j);
+    const int kk = dz > 0 ? kp : (dz < 0 ? km : k);
+    return g.sx * (jj + g.ny * kk);
+  };
+  float4 Y[Q];
+  if (!valid) {
+#pragma unroll
+    for (int q = 0; q < Q; ++q) Y[q] = make_float4(0.f, 0.f, 0.f, 0.f);
+  } else {
+    float E[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      const float* p = a.p[oppq(q)] + row(-cyq(q), -czq(q));
+      Y[q] = __ldg(reinterpret_cast<const float4*>(p + i0));
+      E[q] = 0.f;
+      if (cxq(q) > 0 && xl.edge_prev) E[q] = __ldg(p + i_prev);
+      if (cxq(q) < 0 && xl.edge_next) E[q] = __ldg(p + i_next);
+    }
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      const float4 A = Y[q];
+      if (cxq(q) > 0) {  // elements i0-1 .. i0+2
+        float prev = __shfl_sync(0xffffffffu, A.w, xl.src_prev);
+        if (xl.edge_prev) prev = E[q];
+        Y[q] = make_float4(prev, A.x, A.y, A.z);
+      } else if (cxq(q) < 0) {  // elements i0+1 .. i0+4
+        float next = __shfl_sync(0xffffffffu, A.x, xl.src_next);
+        if (xl.edge_next) next = E[q];
+        Y[q] = make_float4(A.y, A.z, A.w, next);
+      }
+    }
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+      float s[Q];
+#pragma unroll
+      for (int q = 0; q < Q; ++q) s[q] = m == 0 ? Y[q].x : (m == 1 ? Y[q].y : (m == 2 ? Y[q].z : Y[q].w));
+      F32::cell<LES>(s, K);
+#pragma unroll
+      for (int q = 0; q < Q; ++q) {
+        if (m == 0) Y[q].x = s[q];
+        else if (m == 1) Y[q].y = s[q];
+        else if (m == 2) Y[q].z = s[q];
+        else Y[q].w = s[q];
+      }
+    }
+  }
+  __shared__ float xs_last[4][5], xs_first[4][5];
+  bool prev_in = false, next_in = false;
+  int wprev = 0, wnext = 0;
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (tpr >= 32) {
+    const int nw = tpr >> 5, r = pos >> 5;  // warps per row, this warp's place in its row
+    if (nw <= 4) {  // the whole row in this block
+      prev_in = next_in = true;
+      wprev = w - r + (r + nw - 1) % nw;
+      wnext = w - r + (r + 1) % nw;
+    } else {
+      prev_in = w > 0;
+      next_in = w < 3;
+      wprev = w - 1;
+      wnext = w + 1;
+    }
+    if (valid && lane == 31) {
+#pragma unroll
+      for (int q = 0; q < 5; ++q) xs_last[w][q] = Y[q].w;
+    }
+    if (valid && lane == 0) {
+#pragma unroll
+      for (int q = 9; q < 14; ++q) xs_first[w][q - 9] = Y[q].x;
+    }
+  }
+  __syncthreads();
+  if (!valid) return;
+  int js = j, ks = k;  // store rows: recomputed after the collision
+  asm volatile("" : "+r"(js), "+r"(ks));
+  const int jms = js == 0 ? g.ny - 1 : js - 1, jps = js == g.ny - 1 ? 0 : js + 1;
+  const int kms = ks == 0 ? g.nz - 1 : ks - 1, kps = ks == g.nz - 1 ? 0 : ks + 1;
+  auto row_out = [&](int dy, int dz) {
+    const int jj = dy > 0 ? jps : (dy < 0 ? jms : js);
+    const int kk = dz > 0 ? kps : (dz < 0 ? kms : ks);
+    return g.sx * (jj + g.ny * kk);
+  };
+#pragma unroll
+  for (int q = 0; q < Q; ++q) {
+    const float fp = cxq(q) > 0 && xl.edge_prev && prev_in ? xs_last[wprev][q] : 0.f;
+    const float fn = cxq(q) < 0 && xl.edge_next && next_in ? xs_first[wnext][q - 9] : 0.f;
+    shift_out4_f32(Y[q], cxq(q), a.p[q] + row_out(cyq(q), czq(q)), i0, i_prev, i_next, xl, prev_in, next_in, fp, fn);
+  }
+}
+
 // ----------------------------------------------------------------- z-slabs
 // Two-lattice step of one z-slab of a box split along z (the reference's
 // proc_z ranks, SRC/setup_MPI.F90:112-131). x and y wrap in the kernel; a pull
@@ -1519,6 +1659,18 @@ static cudaError_t aa_impl(const Lattice& a, int odd, const StepK& K, int varian
   // per thread at 256^3 (40.5 against 38.9 at 1024^3), the Smagorinsky pair
   // 40.6 against 34.1
   const int lt2 = F::id == FORM_F32 && (variant == 0 || variant == 2) ? vec_log_tpr(a.g, 2) : -1;
+  // FP32 odd step (automatic): four cells per thread where the box fits it;
+  // the pair of AA steps measured 44.1 GLUPS at 256^3 and 44.2 at 512^3
+  // against 42.2 and 40.8 with two cells per thread on both steps, and with
+  // the Smagorinsky collision 43.9 against 40.9 at 256^3 (in FP16 eight cells
+  // gave the Smagorinsky odd step nothing: 76.0 against 76.2, issue-bound)
+  const int lt4f = F::id == FORM_F32 && variant == 0 && odd ? vec_log_tpr(a.g, 4) : -1;
+  if (lt4f >= 0) {
+    const dim3 grid = vec_grid(a.g, lt4f, a.g.nz);
+    if (K.les) k_aa_f32w<true><<<grid, 128, 0, st>>>(pops_of<float>(a), a.g, K, lt4f);
+    else k_aa_f32w<false><<<grid, 128, 0, st>>>(pops_of<float>(a), a.g, K, lt4f);
+    return cudaGetLastError();
+  }
   if (lt2 >= 0) {
     const dim3 grid = vec_grid(a.g, lt2, a.g.nz);
     Pops<float> pf = pops_of<float>(a);

@@ -90,9 +90,9 @@ typedef struct {
   double omega;        /* collision frequency override (e.g. 0 = pure streaming) */
   int extras;          /* 1: bgk_diagnostic also computes enstrophy */
   int kernel;          /* stream-collide kernel: 0 automatic (FP16: 4 where the box
-                          fits, and 8 cells per thread for the BGK odd step of the AA
-                          scheme where the box fits that; FP32: 2 where it fits, else
-                          1), 1 one cell per thread,
+                          fits, FP32: 2 where it fits, else 1; the BGK odd step of the
+                          AA scheme on 8 (FP16) / 4 (FP32) cells per thread where the
+                          box fits that), 1 one cell per thread,
                           2 two cells per thread (FP32 both schemes, FP16 two-lattice),
                           4 four cells per thread (FP16), 8 row pipeline with TMA bulk
                           copies into shared memory (rows up to about 5 KB); boxes a
@@ -103,9 +103,10 @@ typedef struct {
                           per cell Ptotal = |Pi_neq|, Ts = 1/(2 omega) +
                           sqrt(18 cteS^2 Ptotal + (1/omega)^2)/2, relaxation with 1/Ts.
                           0 (default) = plain BGK. The LES collision runs on the one
-                          cell per thread kernels, in FP32 on the two and in FP16 on
-                          the four cells per thread kernels where the box fits (FP16
-                          kernel 2 and kernel 8 fall back);
+                          cell per thread kernels, in FP32 on the two (the AA odd
+                          step: four) and in FP16 on the four cells per thread
+                          kernels where the box fits (FP16 kernel 2 and kernel 8
+                          fall back);
                           bgk_adjoint and bgk_tangent reject it. */
   int proc_z;          /* number of z-slabs the box is split into (the reference's
                           proc_z, SRC/input.F90:41; proc_x = proc_y = 1). 1 (default):

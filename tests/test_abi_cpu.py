@@ -205,8 +205,10 @@ def test_bench_kernel_names_and_shared_config():
     assert bench.kernel_key("fp16", "two_lattice", 256, kernel=1) == "k_two_fp16"
     assert bench.kernel_key("fp16", "two_lattice", 6) == "k_two_fp16"  # rows too short for four cells per thread
     assert bench.kernel_key("fp32", "two_lattice", 256) == "k_two_f32v"
-    assert bench.kernel_key("fp32", "aa", 1024) == "k_aa_f32v"
-    assert bench.kernel_key("fp32", "aa", 256, les=True) == "k_aa_f32v_les"
+    assert bench.kernel_key("fp32", "aa", 1024) == "k_aa_f32w"  # odd step on four cells per thread
+    assert bench.kernel_key("fp32", "aa", 1024, kernel=2) == "k_aa_f32v"
+    assert bench.kernel_key("fp32", "aa", 256, les=True) == "k_aa_f32w_les"
+    assert bench.kernel_key("fp32", "aa", 256, kernel=2, les=True) == "k_aa_f32v_les"
     assert bench.kernel_key("fp32", "aa", 256, kernel=1) == "k_aa_fp32"
     assert bench.kernel_key("fp32", "two_lattice", 24) == "k_two_fp32"  # 12 threads per row: not a power of two
     a = argparse.Namespace(size=256, precision="fp64", scheme="two_lattice", tau=0.505, k0=4.0, kernel=0, les_cs=0.0,

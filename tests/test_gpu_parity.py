@@ -152,6 +152,26 @@ def test_fp16_aa_eight_cells_odd_step_bitexact(bgk, oracle_mod, shape):
         box.close()
 
 
+@pytest.mark.parametrize("les_cs", [0.0, 0.17])
+@pytest.mark.parametrize("shape", [(64, 32, 5), (256, 8, 6), (1024, 4, 3), (2048, 2, 3), (16, 64, 3),
+                                   (8, 128, 3), (4, 256, 2), (128, 16, 8)])
+def test_fp32_aa_four_cells_odd_step_bitexact(bgk, oracle_mod, shape, les_cs):
+    """The automatic FP32 AA odd step with four cells per thread (16-byte
+    chunks; rows of one lane, inside a warp, one and two warps, and eight
+    warps over two blocks with partial chunks at the block boundary), with
+    the BGK and the Smagorinsky collision, gives the oracle's bits over steps
+    of both parities, as does the two-cells kernel (kernel = 2)."""
+    for kernel in (0, 2):
+        orc, box = make_pair(bgk, oracle_mod, shape, "fp32", scheme="aa", kernel=kernel, les_cs=les_cs)
+        orc.set_les(les_cs)
+        for it in range(1, 6):
+            orc.step(0.01, periodic=True)
+            box.col_MC(it)
+            if it in (1, 2, 5):
+                assert same_bits(box.populations(), orc.get_pops()), f"kernel {kernel}, after {it} steps"
+        box.close()
+
+
 @pytest.mark.parametrize("form", ["fp64", "fp32", "fp16"])
 @pytest.mark.parametrize("scheme", ["two_lattice", "aa"])
 @pytest.mark.parametrize("shape", [(5, 7, 9), (64, 16, 8), (33, 20, 7), (256, 3, 2)])

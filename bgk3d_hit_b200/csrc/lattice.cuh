@@ -259,7 +259,7 @@ __device__ __forceinline__ Mom16 moments16_les(const float (&y)[Q], const StepK&
   pt = __fmaf_rn(2.0f * Pxz, Pxz, pt);
   pt = __fmaf_rn(2.0f * Pyz, Pyz, pt);
   const float tau = __fadd_rn(k.tauh_f, __fmul_rn(0.5f, __fsqrt_rn(__fmaf_rn(k.cs18_f, __fsqrt_rn(pt), k.tau2_f))));
-  const float om = __fdiv_rn(1.0f, tau);
+  const float om = __frcp_rn(tau);  // = 1/tau rounded once, as a division would
   om1 = __fsub_rn(1.0f, om);
   const float oms = __fmul_rn(om, k.scale);
 #pragma unroll
